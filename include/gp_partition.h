@@ -1,0 +1,176 @@
+/*
+ * gp_partition.h -- C ABI of the B200-native multilevel k-way graph partitioner.
+ *
+ * The reference (iamrupamroyy/TheGraphPartitioning) is a single executable whose
+ * only entry point is main() in src/gpu_part.cu:878-1390; it has no library API.
+ * The functions below are the library boundary that replaces that executable's
+ * internals:
+ *
+ *   gp_partition / gp_partition_device
+ *       replace the whole V-cycle driven by main(): coarsening loop
+ *       (src/gpu_part.cu:1003-1152), METIS initial partition through the gpmetis
+ *       subprocess (src/gpu_part.cu:803-864, 1157-1185), refinement
+ *       (src/gpu_part.cu:509-759) and projection (src/gpu_part.cu:763-772,
+ *       1205-1274).  The result is the per-vertex part array that the reference
+ *       prints into ./finalpartition.txt (src/gpu_part.cu:1296-1322).
+ *   gp_edge_cut_device
+ *       replaces computeEdgeCut / compute_edgecut (src/gpu_part.cu:400-469),
+ *       with an int64 accumulator instead of the reference's int32.
+ *   gp_last_error
+ *       replaces the reference's CUDA_CHECK -> exit(EXIT_FAILURE) convention
+ *       (src/gpu_part.cu:40-47): nothing in this library exits the process.
+ *
+ * Graph contract (same as the files written by preprocess/conversion.py:66-93):
+ * 0-based CSR, symmetric, no self-loops.  rowptr has n+1 int64 entries, colidx
+ * and ewgt have rowptr[n] entries.  vwgt/ewgt may be NULL (unit weights).
+ * All weights must be >= 1; the sum of vertex weights and the sum of directed
+ * edge weights must each fit in int32 (so that every coarse weight, every
+ * part-connectivity count and every gain is an exact int32).
+ *
+ * Every function returns GP_OK (0) or a negative GP_E* code and never exits.
+ * gp_last_error() returns a thread-local message describing the last failure.
+ */
+#ifndef GP_PARTITION_H
+#define GP_PARTITION_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GP_OK        0
+#define GP_EINVAL   -1   /* invalid argument or malformed graph                 */
+#define GP_ENOMEM   -2   /* device or host allocation failed                    */
+#define GP_ECUDA    -3   /* a CUDA runtime call or kernel launch failed         */
+#define GP_ETIMEOUT -4   /* a bounded device wait gave up                       */
+#define GP_EINTERNAL -5  /* internal consistency check failed                   */
+
+#define GP_MAX_K 1024    /* largest supported number of parts                   */
+
+#define GP_OPTIONS_VERSION 1
+
+/* Tunables of the deterministic V-cycle.  Zero in any field selects the
+ * default; gp_default_options() fills the defaults explicitly.  The CPU oracle
+ * reads the same structure, so a given (graph, k, imbalance, seed, options)
+ * produces the same partition on both. */
+typedef struct gp_options {
+    int32_t version;            /* GP_OPTIONS_VERSION                                   */
+    int32_t coarsen_to;         /* stop coarsening at <= this many vertices (0: auto)   */
+    int32_t match_rounds;       /* max handshake rounds per level (default 8)           */
+    int32_t two_hop;            /* >0 or 0: pair leftovers sharing an anchor; <0: off   */
+    int32_t init_trials;        /* initial-partition trials (default 64)                */
+    int32_t refine_max_iters;   /* max refinement iterations per level (default 64)     */
+    int32_t refine_patience;    /* stop after this many non-improving iterations (12)   */
+    int32_t lp_filter_den;      /* negative-gain filter: -gain < conn_own/den (4)      */
+    int32_t strong_after;       /* consecutive rebalance iterations before strong (2)  */
+    int32_t check_input;        /* 0/1: structural checks, 2: +symmetry, <0: none        */
+    int32_t verbose;            /* 0: silent                                           */
+    int32_t reserved[5];
+} gp_options;
+
+/* Result record of one call. */
+typedef struct gp_stats {
+    int64_t cut;                /* exact edge cut of the returned partition (int64)     */
+    int64_t max_part_weight;
+    int64_t total_weight;       /* sum of vertex weights                               */
+    int64_t max_allowed;        /* floor((1+imbalance) * total_weight / k)             */
+    double  imbalance;          /* max_part_weight * k / total_weight - 1               */
+    int32_t levels;             /* number of graphs in the hierarchy (>= 1)            */
+    int32_t coarsest_n;
+    int32_t best_trial;         /* initial-partition trial that was kept               */
+    int32_t refine_iters;       /* refinement iterations over all levels               */
+    int64_t algo_bytes;         /* algorithmic HBM bytes of all executed passes        */
+    int64_t kernel_launches;    /* kernels this call launched                          */
+    double  ms_coarsen;         /* device time per phase (CUDA events)                 */
+    double  ms_initial;
+    double  ms_refine;
+    double  ms_project;
+    double  ms_total;
+    double  ms_h2d;             /* host API only: host->device copies                  */
+    double  ms_d2h;
+} gp_stats;
+
+/* ---- optional tracing (tests): host copies of intermediate results ----- */
+enum gp_trace_kind {
+    GP_TR_MATCH = 1,       /* a0 = match[n]   (partner or -1)                        */
+    GP_TR_CONTRACT = 2,    /* a0 = cmap[n]; coarse graph in rowptr/colidx/ewgt/vwgt   */
+    GP_TR_INITPART = 3,    /* a0 = part[n] of the kept trial; iter = trial id        */
+    GP_TR_REFINE_ITER = 4, /* a0 = dest[n] (-1: no proposal), a1 = gain[n],
+                              a2 = part[n] after the iteration; cut/maxpw before it   */
+    GP_TR_LEVEL_DONE = 5   /* a0 = part[n] after refinement of this level             */
+};
+
+typedef struct gp_trace_event {
+    int32_t kind;
+    int32_t level;          /* 0 = input graph                                     */
+    int32_t iter;
+    int32_t mode;           /* refine: 0 label propagation, 1 weak, 2 strong rebalance */
+    int64_t n;
+    int64_t m;              /* directed entries of the graph the arrays refer to     */
+    int64_t cut;
+    int64_t maxpw;
+    int64_t count;          /* pairs matched / moves applied                         */
+    const int32_t* a0;
+    const int32_t* a1;
+    const int32_t* a2;
+    const int64_t* rowptr;  /* GP_TR_CONTRACT: the coarse graph                     */
+    const int32_t* colidx;
+    const int32_t* ewgt;
+    const int32_t* vwgt;
+} gp_trace_event;
+
+typedef void (*gp_trace_fn)(void* user, const gp_trace_event* ev);
+
+/* Fill *opt with the defaults. */
+int gp_default_options(gp_options* opt);
+
+/* Partition a host-resident graph into k parts.  part_out: n int32 (host).
+ * Copies the graph to the current CUDA device, runs the V-cycle there and
+ * copies the part array back.  Synchronous. */
+int gp_partition(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                 const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                 float imbalance, uint64_t seed, int32_t* part_out);
+
+/* Same with options, statistics and tracing (any of the three may be NULL). */
+int gp_partition_ex(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                    const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                    float imbalance, uint64_t seed, int32_t* part_out,
+                    const gp_options* opt, gp_stats* stats,
+                    gp_trace_fn trace, void* trace_user);
+
+/* Device-pointer variant: every array lives in device memory of the current
+ * device; work is ordered on `stream` (a cudaStream_t, NULL = legacy default
+ * stream).  Returns once the partition is written (the call synchronizes the
+ * stream).  One call in flight per device at a time: calls from several host
+ * threads are serialized on a per-device lock. */
+int gp_partition_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                        const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t k,
+                        float imbalance, uint64_t seed, int32_t* d_part_out,
+                        void* stream, const gp_options* opt, gp_stats* stats,
+                        gp_trace_fn trace, void* trace_user);
+
+/* Exact edge cut of a partition (device pointers).  *cut_out and
+ * part_weights_out (k int64, may be NULL) are written to HOST memory.
+ * Mirrors computeEdgeCut (src/gpu_part.cu:433-469) but accumulates in int64
+ * and does not divide a possibly odd sum: it counts each undirected edge once
+ * by summing directed cross entries and halving an even total. */
+int gp_edge_cut_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                       const int32_t* d_ewgt, const int32_t* d_vwgt,
+                       const int32_t* d_part, int32_t k, void* stream,
+                       int64_t* cut_out, int64_t* part_weights_out);
+
+/* Release cached device workspaces of the current device. */
+int gp_release_workspace(void);
+
+/* Thread-local description of the last error ("" when none). */
+const char* gp_last_error(void);
+
+/* Library version string. */
+const char* gp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GP_PARTITION_H */

@@ -1,0 +1,115 @@
+"""GPU parity: the sm_100a library against the CPU oracle, bit-exact.
+
+Every case runs the full V-cycle on both sides with tracing on and compares,
+event by event: the matching of every level, the fine->coarse map and coarse
+CSR (ids, weights, vertex weights), the kept initial-partition trial, each
+refinement iteration's proposals (destination, gain), its resulting partition
+and the cut/heaviest-part before it, and the partition after each level.
+"""
+import numpy as np
+import pytest
+import torch
+
+from thegraphpartitioning_b200 import graphs
+from helpers import compare_traces, star_plus_grid, to_np, weighted
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    yield "grid64_k4", graphs.grid2d(64, 64), 4, 0.03, None, {}
+    yield "grid48x80_k7", graphs.grid2d(48, 80), 7, 0.05, None, {}
+    yield "rmat12_k16", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {}
+    yield "chunglu_k8", graphs.chung_lu(12000, 40000, seed=2), 8, 0.03, None, {}
+    yield "grid3d_k32", graphs.grid3d(16, 16, 16), 32, 0.03, None, {}
+    yield "weighted_k5", graphs.grid2d(40, 50), 5, 0.05, "w", {}
+    yield "star_heavy_k4", star_plus_grid(), 4, 0.03, None, {"coarsen_to": 200}
+    yield "rmat11_k64_tight", graphs.rmat(11, seed=3)[:2], 64, 0.0, None, {}
+    yield "er_k3_nohop", graphs.erdos_renyi(3000, 3.0, seed=5), 3, 0.02, None, {"two_hop": -1}
+    yield "rgg_k2", graphs.random_geometric(4000, 8.0, seed=6), 2, 0.03, None, {"init_trials": 8}
+
+
+CASES = list(_cases())
+
+
+@pytest.mark.parametrize("name,g,k,imb,w,opts", CASES, ids=[c[0] for c in CASES])
+def test_trace_parity(oracle_mod, gp, cuda, name, g, k, imb, w, opts):
+    rp, ci = to_np(*g)
+    ew = vw = None
+    if w:
+        ew, vw = weighted(rp, ci, seed=9)
+    seed = 11
+    p_ref, s_ref, ev_ref = oracle_mod.partition(rp, ci, k, imb, seed, vwgt=vw, ewgt=ew, options=opts, trace=True)
+    # device entry point through torch CUDA tensors
+    d = lambda a: None if a is None else torch.from_numpy(a).to(cuda)
+    p_gpu, s_gpu, ev_gpu = gp.partition(d(rp), d(ci), k, imb, seed, vwgt=d(vw), ewgt=d(ew), options=opts, trace=True)
+    compare_traces(ev_ref, ev_gpu)
+    assert np.array_equal(p_ref, p_gpu.cpu().numpy())
+    for key in ("cut", "max_part_weight", "total_weight", "max_allowed", "levels", "coarsest_n",
+                "best_trial", "refine_iters"):
+        assert s_ref[key] == s_gpu[key], (key, s_ref[key], s_gpu[key])
+
+
+def test_host_entry_point_matches_oracle(oracle_mod, gp, cuda):
+    rp, ci = to_np(*graphs.rmat(13, seed=2)[:2])
+    p_ref, s_ref, _ = oracle_mod.partition(rp, ci, 32, 0.03, 5)
+    p_gpu, s_gpu, _ = gp.partition(rp, ci, 32, 0.03, 5)
+    assert np.array_equal(p_ref, p_gpu)
+    assert s_ref["cut"] == s_gpu["cut"]
+
+
+def test_edge_cut_device(oracle_mod, gp, cuda):
+    rp, ci = to_np(*graphs.chung_lu(30000, 100000, seed=4))
+    ew, vw = weighted(rp, ci, seed=1)
+    k = 13
+    part = (np.arange(len(rp) - 1) * 7919 % k).astype(np.int32)
+    cut_ref, pw_ref = oracle_mod.edge_cut(rp, ci, part, k, ewgt=ew, vwgt=vw)
+    d = lambda a: torch.from_numpy(a).to(cuda)
+    cut, pw = gp.edge_cut(d(rp), d(ci), d(part), k, ewgt=d(ew), vwgt=d(vw))
+    assert cut == cut_ref
+    assert np.array_equal(pw, pw_ref)
+
+
+def test_determinism_repeated_calls(gp, cuda):
+    rp, ci = graphs.rmat(14, seed=7)[:2]
+    rp, ci = rp.to(cuda), ci.to(cuda)
+    outs = [gp.partition(rp, ci, 64, 0.03, 3)[0].cpu().numpy() for _ in range(3)]
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+@pytest.mark.parametrize("case", ["self", "range", "rowptr", "weight", "asym", "k0", "kbig"])
+def test_device_rejects_invalid(gp, cuda, case):
+    rp, ci = to_np(*graphs.grid2d(6, 6))
+    k, ew, opts = 2, None, None
+    if case == "self":
+        ci = ci.copy(); ci[0] = 0
+    elif case == "range":
+        ci = ci.copy(); ci[3] = 99
+    elif case == "rowptr":
+        rp = rp.copy(); rp[5] = rp[7]
+    elif case == "weight":
+        ew = np.ones(len(ci), np.int32); ew[2] = 0
+    elif case == "asym":
+        rp = np.array([0, 2, 4, 4, 5, 6]); ci = np.array([1, 2, 0, 3, 4, 2], np.int32)
+        opts = {"check_input": 2}
+    elif case == "k0":
+        k = 0
+    elif case == "kbig":
+        k = 37
+    d = lambda a: None if a is None else torch.from_numpy(np.asarray(a)).to(cuda)
+    with pytest.raises(gp.GPError) as ei:
+        gp.partition(d(rp.astype(np.int64)), d(ci.astype(np.int32)), k, 0.03, ewgt=d(ew), options=opts)
+    assert ei.value.code == -1
+    # the context is still usable afterwards
+    rp2, ci2 = graphs.grid2d(8, 8)
+    p, st, _ = gp.partition(rp2.to(cuda), ci2.to(cuda), 4)
+    assert st["cut"] >= 16
+
+
+def test_full_size_grid_config(oracle_mod, gp, cuda):
+    """512x512 grid, k=4, 3%: identical to the oracle at full size."""
+    rp, ci = to_np(*graphs.grid2d(512, 512))
+    p_ref, s_ref, _ = oracle_mod.partition(rp, ci, 4, 0.03, 0)
+    p_gpu, s_gpu, _ = gp.partition(torch.from_numpy(rp).to(cuda), torch.from_numpy(ci).to(cuda), 4, 0.03, 0)
+    assert np.array_equal(p_ref, p_gpu.cpu().numpy())
+    assert s_gpu["max_part_weight"] <= s_gpu["max_allowed"]

@@ -1,0 +1,163 @@
+"""B200-native multilevel k-way graph partitioner.
+
+Python binding of the C ABI in include/gp_partition.h (libgp_b200.so, built
+in-tree by `make -C thegraphpartitioning_b200/csrc`).  There is no CPU
+fallback: if the library is missing, every call raises.
+
+    part, stats, _ = partition(rowptr, colidx, k)            # host arrays
+    part, stats, _ = partition(d_rowptr, d_colidx, k)        # torch CUDA tensors
+
+The reference (iamrupamroyy/TheGraphPartitioning) exposes the same operation
+only as the `gpu_part` executable (src/gpu_part.cu:878); that CLI is rebuilt
+as bin/gpu_part on top of this library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (
+    GpOptions, GpStats, TraceCollector, make_options, i32p, i64p, ERROR_NAMES,
+)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgp_b200.so")
+CLI_PATH = os.path.join(HERE, "bin", "gpu_part")
+_lib = None
+
+
+class GPError(RuntimeError):
+    """A GP_E* status returned by the library."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def build() -> None:
+    import subprocess
+    subprocess.run(["make", "-C", os.path.join(HERE, "csrc"), "-s", "-j8"], check=True)
+
+
+def lib():
+    """Load libgp_b200.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {os.path.join(HERE, 'csrc')}` "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+    L.gp_partition.restype = C.c_int
+    L.gp_partition.argtypes = [C.c_int64, P64, P32, P32, P32, C.c_int32, C.c_float, C.c_uint64, P32]
+    L.gp_partition_ex.restype = C.c_int
+    L.gp_partition_ex.argtypes = [C.c_int64, P64, P32, P32, P32, C.c_int32, C.c_float, C.c_uint64, P32,
+                                  C.POINTER(GpOptions), C.POINTER(GpStats), C.c_void_p, C.c_void_p]
+    L.gp_partition_device.restype = C.c_int
+    L.gp_partition_device.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                      C.c_float, C.c_uint64, C.c_void_p, C.c_void_p, C.POINTER(GpOptions),
+                                      C.POINTER(GpStats), C.c_void_p, C.c_void_p]
+    L.gp_edge_cut_device.restype = C.c_int
+    L.gp_edge_cut_device.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_int32, C.c_void_p, P64, P64]
+    L.gp_default_options.restype = C.c_int
+    L.gp_default_options.argtypes = [C.POINTER(GpOptions)]
+    L.gp_release_workspace.restype = C.c_int
+    L.gp_last_error.restype = C.c_char_p
+    L.gp_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise GPError(rc, lib().gp_last_error().decode())
+
+
+def _opts(options):
+    if options is None:
+        return make_options()
+    if isinstance(options, GpOptions):
+        return options
+    return make_options(**options)
+
+
+def _is_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(x.is_cuda)
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def partition(rowptr, colidx, k: int, imbalance: float = 0.03, seed: int = 0, vwgt=None, ewgt=None,
+              options=None, trace: bool = False, out=None, stream=None):
+    """Partition a CSR graph into k parts.
+
+    Host inputs (numpy / lists / CPU tensors) go through gp_partition_ex (the
+    library copies them to the current device).  torch CUDA tensors go through
+    gp_partition_device on `stream` (default: torch's current stream); the
+    result is then a CUDA int32 tensor (written into `out` when given).
+    Returns (part, stats: dict, trace_events: list)."""
+    L = lib()
+    opt = _opts(options)
+    st = GpStats()
+    col = TraceCollector() if trace else None
+    tfn = C.cast(col.cfunc, C.c_void_p) if col else None
+    seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    if _is_cuda(rowptr):
+        import torch
+        n = rowptr.numel() - 1
+        assert rowptr.dtype == torch.int64 and colidx.dtype == torch.int32
+        for t in (rowptr, colidx, vwgt, ewgt):
+            if t is not None:
+                assert t.is_cuda and t.is_contiguous()
+        part = out if out is not None else torch.empty(max(n, 0), dtype=torch.int32, device=rowptr.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+        rc = L.gp_partition_device(n, _ptr(rowptr), _ptr(colidx), _ptr(vwgt), _ptr(ewgt), int(k), float(imbalance),
+                                   seed, _ptr(part), C.c_void_p(stream), C.byref(opt), C.byref(st), tfn, None)
+        _check(rc)
+        return part, st.as_dict(), (col.events if col else [])
+    rp = np.ascontiguousarray(np.asarray(rowptr), dtype=np.int64)
+    ci = np.ascontiguousarray(np.asarray(colidx), dtype=np.int32)
+    vw = None if vwgt is None else np.ascontiguousarray(np.asarray(vwgt), dtype=np.int32)
+    ew = None if ewgt is None else np.ascontiguousarray(np.asarray(ewgt), dtype=np.int32)
+    n = len(rp) - 1
+    part = np.zeros(max(n, 1), dtype=np.int32)
+    rc = L.gp_partition_ex(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance), seed, i32p(part),
+                           C.byref(opt), C.byref(st), tfn, None)
+    _check(rc)
+    return part[:n], st.as_dict(), (col.events if col else [])
+
+
+def edge_cut(rowptr, colidx, part, k: int, ewgt=None, vwgt=None, stream=None):
+    """Exact (cut, part_weights) of a partition held in torch CUDA tensors."""
+    import torch
+    L = lib()
+    n = rowptr.numel() - 1
+    cut = C.c_int64(0)
+    pw = np.zeros(int(k), dtype=np.int64)
+    if stream is None:
+        stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+    rc = L.gp_edge_cut_device(n, _ptr(rowptr), _ptr(colidx), _ptr(ewgt), _ptr(vwgt), _ptr(part), int(k),
+                              C.c_void_p(stream), C.byref(cut), i64p(pw))
+    _check(rc)
+    return int(cut.value), pw
+
+
+def default_options() -> GpOptions:
+    o = GpOptions()
+    _check(lib().gp_default_options(C.byref(o)))
+    return o
+
+
+def release_workspace() -> None:
+    _check(lib().gp_release_workspace())
+
+
+def version() -> str:
+    return lib().gp_version().decode()

@@ -1,0 +1,147 @@
+// gp_common.cuh -- shared definitions of the B200 partitioner library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+#include "../../include/gp_partition.h"
+
+namespace gp {
+
+// ---------------------------------------------------------------- errors
+// Library code throws GpError internally; the C-ABI entry points catch it and
+// turn it into a return code plus gp_last_error() text.  Nothing exits.
+struct GpError : std::runtime_error {
+    int code;
+    GpError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define GP_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess)                                                     \
+            throw ::gp::GpError(e_ == cudaErrorMemoryAllocation ? GP_ENOMEM : GP_ECUDA, \
+                                std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GP_LAUNCHED(ctx)                                                           \
+    do {                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                       \
+        if (e_ != cudaSuccess)                                                     \
+            throw ::gp::GpError(GP_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+        (ctx).launches++;                                                          \
+    } while (0)
+
+// ---------------------------------------------------------------- rules
+// The deterministic rule set shared with the CPU oracle (oracle/oracle.cpp
+// restates the same functions independently).
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    // splitmix64 finalizer (published constants of Stafford's Mix13)
+    x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ULL;
+    x ^= x >> 27; x *= 0x94d049bb133111ebULL;
+    x ^= x >> 31; return x;
+}
+__host__ __device__ __forceinline__ uint64_t level_salt(uint64_t seed, int level) {
+    return mix64(seed ^ mix64(0x9E3779B97F4A7C15ULL * (uint64_t)(level + 1)));
+}
+__host__ __device__ __forceinline__ uint64_t trial_salt(uint64_t seed, int t) {
+    return mix64(seed ^ mix64(0xD1B54A32D192ED03ULL * (uint64_t)(t + 1)));
+}
+__host__ __device__ __forceinline__ uint64_t depth_salt(uint64_t tsalt, int d) {
+    return mix64(tsalt ^ mix64(0x8CB92BA72F3D8DD7ULL * (uint64_t)(d + 1)));
+}
+__host__ __device__ __forceinline__ uint32_t edge_hash(uint64_t salt, int32_t a, int32_t b) {
+    uint32_t lo = (uint32_t)(a < b ? a : b), hi = (uint32_t)(a < b ? b : a);
+    return (uint32_t)(mix64(salt ^ (((uint64_t)lo << 32) | hi)) >> 32);
+}
+__host__ __device__ __forceinline__ uint64_t edge_key(int32_t w, uint32_t h) {
+    return ((uint64_t)(uint32_t)w << 32) | h;
+}
+__host__ __device__ __forceinline__ uint32_t mag_bucket(uint32_t x) {
+    if (x < 64) return x;
+#ifdef __CUDA_ARCH__
+    int e = 31 - __clz(x);
+#else
+    int e = 31 - __builtin_clz(x);
+#endif
+    uint32_t mant = (x >> (e - 4)) & 15u;
+    return 64u + (uint32_t)(e - 6) * 16u + mant;
+}
+__host__ __device__ __forceinline__ uint32_t loss_bucket(int32_t loss) {
+    if (loss >= 0) return 480u + mag_bucket((uint32_t)loss);
+    return 480u - mag_bucket((uint32_t)(-(int64_t)loss));
+}
+
+// ---------------------------------------------------------------- arena
+// Grow-only device memory cache.  A call bump-allocates from chunks; when a
+// call needed more than one chunk, the chunks are merged into one at the end
+// so that the next call of the same size allocates nothing.
+class Arena {
+public:
+    ~Arena() { release(); }
+    void* alloc(size_t bytes);
+    void reset();            // forget all allocations of the call
+    size_t mark() const { return used_total_; }
+    void release();          // free device memory
+    void consolidate();      // merge chunks after a call
+    size_t capacity() const;
+    // stack-like scratch: restore to an earlier mark (only within the last chunk)
+    struct Mark { size_t chunk, off, total; };
+    Mark save() const { return Mark{cur_, chunks_.empty() ? 0 : chunks_[cur_].off, used_total_}; }
+    void restore(const Mark& m);
+private:
+    struct Chunk { char* p; size_t size; size_t off; };
+    std::vector<Chunk> chunks_;
+    size_t cur_ = 0;
+    size_t used_total_ = 0;
+    size_t peak_total_ = 0;
+};
+
+// ---------------------------------------------------------------- context
+struct Ctx {
+    cudaStream_t s = nullptr;
+    Arena* keep = nullptr;     // lives for the whole call (hierarchy)
+    Arena* tmp = nullptr;      // scratch, restored after each step
+    int64_t launches = 0;
+    int64_t bytes = 0;         // algorithmic bytes of executed passes
+    int sm_count = 148;
+    int64_t* h_pinned = nullptr;  // small pinned staging buffer (64 int64)
+    template <class T> T* keep_alloc(int64_t count) { return (T*)keep->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
+    template <class T> T* tmp_alloc(int64_t count) { return (T*)tmp->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
+    void sync() { GP_CUDA(cudaStreamSynchronize(s)); }
+};
+
+// Device-side view of one level of the hierarchy.
+struct DGraph {
+    int64_t n = 0, m = 0;
+    const int64_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const int32_t* ew = nullptr;   // nullptr = unit
+    const int32_t* vw = nullptr;   // nullptr = unit
+};
+
+// ---------------------------------------------------------------- launch helpers
+inline int grid_for(int64_t items, int per_block, int cap = 148 * 16) {
+    int64_t g = (items + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+constexpr int kHeavyDeg = 2048;   // rows longer than this take a whole CTA
+
+// ---------------------------------------------------------------- primitives (gp_prims.cu)
+// exclusive scan; out may alias in; returns total on the host if total_out != nullptr
+void scan_excl_i32_to_i64(Ctx& c, const int32_t* in, int64_t* out, int64_t n, int64_t* d_total);
+void scan_excl_i64(Ctx& c, const int64_t* in, int64_t* out, int64_t n, int64_t* d_total);
+// LSD radix sort of (key, val) pairs by the low `bits` bits of key.  Result in
+// keys/vals (ping-pong through the provided temporaries).
+void radix_sort_pairs(Ctx& c, uint64_t* keys, int32_t* vals, uint64_t* keys_tmp, int32_t* vals_tmp,
+                      int64_t n, int bits);
+int64_t read_i64(Ctx& c, const int64_t* d);   // synchronous small read
+void memset_async(Ctx& c, void* p, int value, size_t bytes);
+
+}  // namespace gp

@@ -1,0 +1,101 @@
+// gp_internal.cuh -- declarations shared by the library's translation units.
+#pragma once
+
+#include "gp_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace gp {
+
+struct Params {
+    int32_t k = 2;
+    int64_t W = 0;        // total vertex weight
+    int64_t Lmax = 0;     // max allowed part weight
+    int64_t maxvw = 0;    // coarse vertex weight cap
+    uint64_t seed = 0;
+    float imbalance = 0.03f;
+    gp_options o{};
+};
+
+struct Level {
+    DGraph g;
+    int32_t* cmap = nullptr;      // fine -> coarse map to the next coarser level
+    int32_t* heavy = nullptr;     // vertices with degree > kHeavyDeg
+    int64_t nheavy = 0;
+    // bytes of one neighbour scan: row pointers, column ids, weights, gathered per-neighbour int32 state
+    int64_t scan_bytes() const { return 8 * (g.n + 1) + 4 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.m; }
+};
+
+// Host-side rule helpers (identical to the oracle's).
+inline void resolve_options(const gp_options* in, int32_t k, gp_options* o) {
+    gp_options d;
+    memset(&d, 0, sizeof d);
+    if (in) d = *in;
+    d.version = GP_OPTIONS_VERSION;
+    if (d.coarsen_to <= 0) d.coarsen_to = (int32_t)std::max<int64_t>(1024, 32LL * k);
+    if (d.match_rounds <= 0) d.match_rounds = 8;
+    if (d.two_hop == 0) d.two_hop = 1;
+    if (d.init_trials <= 0) d.init_trials = 64;
+    if (d.refine_max_iters <= 0) d.refine_max_iters = 64;
+    if (d.refine_patience <= 0) d.refine_patience = 12;
+    if (d.lp_filter_den <= 0) d.lp_filter_den = 4;
+    if (d.strong_after <= 0) d.strong_after = 2;
+    if (d.check_input == 0) d.check_input = 1;
+    *o = d;
+}
+
+inline int64_t compute_lmax(int64_t W, int32_t k, float imbalance) {
+    double lim = (1.0 + (double)imbalance) * (double)W / (double)k;
+    int64_t l = (int64_t)std::floor(lim);
+    int64_t avg = (W + k - 1) / k;
+    return std::max(l, avg);
+}
+
+struct Tracer {
+    gp_trace_fn fn = nullptr;
+    void* user = nullptr;
+    bool on() const { return fn != nullptr; }
+    void emit(const gp_trace_event& e) const { if (fn) fn(user, &e); }
+};
+
+// refinement buffers sized for the finest level
+struct RefineBufs {
+    int32_t* part = nullptr;
+    int32_t* part_next = nullptr;
+    int32_t* best = nullptr;
+    int32_t* dest = nullptr;
+    int32_t* gain = nullptr;
+    uint8_t* lock = nullptr;
+    uint8_t* lock_next = nullptr;
+    int64_t* pw = nullptr;        // k
+    int64_t* best_pw = nullptr;   // k
+    int64_t* status = nullptr;    // 16
+    int32_t* clist = nullptr;     // LP candidates (light rows)
+    uint64_t* ckeys = nullptr;    // rebalance candidate keys
+    int32_t* cvals = nullptr;
+    uint64_t* ckeys2 = nullptr;
+    int32_t* cvals2 = nullptr;
+};
+
+// device status block of the refinement loop; slots [0, S_NRESET) are cleared
+// before every connectivity pass, S_STEP_MOVES before every move step
+enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NCAND = 3, S_LIGHT = 5, S_NLIST = 6, S_CDEG = 7,
+                  S_NRESET = 8, S_STEP_MOVES = 8, S_NSLOTS = 16 };
+
+// gp_coarsen.cu
+void build_heavy(Ctx& c, Level& L);
+int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out);
+void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match);
+
+// gp_initpart.cu
+int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out);
+
+// gp_refine.cu
+int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr);
+void project(Ctx& c, const Level& fine, const int32_t* part_coarse, int32_t* part_fine);
+void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* pw);
+void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw);
+
+}  // namespace gp

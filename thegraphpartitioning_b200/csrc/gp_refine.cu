@@ -1,0 +1,631 @@
+// gp_refine.cu -- gain refinement, rebalancing and projection.
+//
+// Replaces deterministicRefinement (src/gpu_part.cu:509-759) with its kernels
+// computeGainsAndDestinations, markCandidates, tokenPassing,
+// bufferCandidateMoves, computeAvailableCapacity, bitonicSortStep/customSortMoves,
+// selectMoves, commitMoves (src/gpu_part.cu:258-397, 472-506), the edge-cut
+// kernel (src/gpu_part.cu:400-423) and kwayMapCoarseToFine (src/gpu_part.cu:763-772).
+//
+// One refinement iteration:
+//   k_conn      one pass over every row: exact int32 part-connectivity histogram
+//               in shared memory (warp-private for rows <= kHeavyDeg, CTA-wide
+//               for longer rows), cut contribution of every vertex (so the cut
+//               of the current state costs no extra pass), and the move proposal
+//               of the mode the device derives from the part weights
+//               (label propagation when no part exceeds Lmax, else rebalancing).
+//   LP:         k_copy_state + k_lp_apply: each candidate re-evaluates its gain
+//               against the proposals of higher-priority neighbours
+//               ((gain desc, id asc)) and moves when that gain is >= 0;
+//               double-buffered part/lock arrays, part-weight deltas aggregated
+//               per CTA in shared memory.
+//   rebalance:  candidates (keys = source | loss bucket | id) are radix sorted,
+//               exclusive prefix sums of vertex weight select the moves that
+//               cover each source's excess and fit each destination's capacity
+//               (weak) or the concatenated free capacities (strong).
+#include "gp_internal.cuh"
+
+#include <cstring>
+
+namespace gp {
+
+constexpr int RT = 256;              // threads per CTA
+constexpr int RW = RT / 32;          // warps per CTA
+enum { MODE_LP = 0, MODE_RB = 1, MODE_EVAL = 2 };
+
+__device__ __forceinline__ void argmax_q(uint64_t& bk, int32_t& bq, uint64_t k2, int32_t q2) {
+    if (k2 > bk || (k2 == bk && (uint32_t)q2 < (uint32_t)bq)) { bk = k2; bq = q2; }
+}
+__device__ __forceinline__ void warp_argmax_q(uint64_t& bk, int32_t& bq) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
+        int32_t q2 = __shfl_xor_sync(0xffffffffu, bq, o);
+        argmax_q(bk, bq, k2, q2);
+    }
+}
+template <class T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// LP candidate rule: gain >= 0, or -gain < own/den
+__device__ __forceinline__ bool lp_candidate(int64_t g, int64_t own, int32_t den) {
+    return g >= 0 || -g < own / den;
+}
+
+// ------------------------------------------------------------------ k_conn
+// status: [S_CROSS] += directed cross weight, [S_MAXPW], [S_MODE], [S_LIGHT] written by CTA 0,
+// [S_NCAND] rebalance candidates appended to ckeys/cvals, [S_NLIST] LP candidates appended to clist.
+__global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, int32_t den, int force_eval,
+                                             const int32_t* __restrict__ part, const uint8_t* __restrict__ lock,
+                                             const int64_t* __restrict__ pw, const int32_t* __restrict__ heavy,
+                                             int64_t nheavy, int32_t* __restrict__ dest, int32_t* __restrict__ gain,
+                                             int64_t* __restrict__ status, uint64_t* __restrict__ ckeys,
+                                             int32_t* __restrict__ cvals, int32_t* __restrict__ clist) {
+    extern __shared__ int32_t csm[];
+    const int kpad = (k + 15) & ~15;
+    uint8_t* over = (uint8_t*)csm;
+    int32_t* hist_all = csm + kpad / 4;
+    __shared__ int64_t s_red[RW];
+    __shared__ uint64_t s_k[RW];
+    __shared__ int32_t s_q[RW];
+    __shared__ int64_t s_maxpw;
+    __shared__ int32_t s_light;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+
+    // over flags, heaviest part, lightest non-overweight part (ties: lower id)
+    int64_t mx = 0;
+    uint64_t lk = 0; int32_t lq = -1;  // argmax of (~pw) == argmin pw
+    for (int q = threadIdx.x; q < k; q += RT) {
+        const int64_t x = pw[q];
+        over[q] = x > Lmax;
+        mx = x > mx ? x : mx;
+        if (x <= Lmax) argmax_q(lk, lq, ~(uint64_t)x, q);
+    }
+    for (int i = threadIdx.x; i < RW * k; i += RT) hist_all[i] = 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) { int64_t y = __shfl_xor_sync(0xffffffffu, mx, o); mx = y > mx ? y : mx; }
+    warp_argmax_q(lk, lq);
+    if (lane == 0) { s_red[w] = mx; s_k[w] = lk; s_q[w] = lq; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t m2 = 0; uint64_t k2 = 0; int32_t q2 = -1;
+        for (int i = 0; i < RW; ++i) { m2 = s_red[i] > m2 ? s_red[i] : m2; argmax_q(k2, q2, s_k[i], s_q[i]); }
+        s_maxpw = m2; s_light = q2;
+    }
+    __syncthreads();
+    const int64_t maxpw = s_maxpw;
+    const int32_t light = s_light;
+    const int mode = force_eval ? MODE_EVAL : (maxpw > Lmax ? MODE_RB : MODE_LP);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        status[S_MAXPW] = maxpw; status[S_MODE] = mode; status[S_LIGHT] = light;
+    }
+    int64_t acc = 0;  // directed cross weight (this thread)
+
+    if ((int64_t)blockIdx.x < nheavy) {
+        // ---- one long row per CTA
+        int32_t* hist = hist_all;
+        const int64_t v = heavy[blockIdx.x];
+        const int32_t p = part[v];
+        const bool active = (mode == MODE_LP && !lock[v]) || (mode == MODE_RB && over[p]);
+        const int64_t beg = g.rp[v], end = g.rp[v + 1];
+        int64_t cross = 0, tot = 0;
+        for (int64_t e = beg + threadIdx.x; e < end; e += RT) {
+            const int32_t q = part[g.ci[e]];
+            const int32_t wt = g.ew ? g.ew[e] : 1;
+            tot += wt;
+            if (q != p) cross += wt;
+            if (active) atomicAdd(&hist[q], wt);
+        }
+        cross = warp_sum(cross); tot = warp_sum(tot);
+        __syncthreads();
+        if (lane == 0) { s_red[w] = cross; s_k[w] = (uint64_t)tot; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t c2 = 0, t2 = 0;
+            for (int i = 0; i < RW; ++i) { c2 += s_red[i]; t2 += (int64_t)s_k[i]; }
+            s_red[0] = c2; s_k[0] = (uint64_t)t2;
+        }
+        __syncthreads();
+        cross = s_red[0]; tot = (int64_t)s_k[0];
+        __syncthreads();
+        uint64_t bk = 0; int32_t bq = -1;
+        if (active)
+            for (int q = threadIdx.x; q < k; q += RT)
+                if (q != p && hist[q] > 0 && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+        warp_argmax_q(bk, bq);
+        if (lane == 0) { s_k[w] = bk; s_q[w] = bq; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = 1; i < RW; ++i) argmax_q(bk, bq, s_k[i], s_q[i]);
+            acc += cross;
+            const int64_t own = tot - cross;
+            int32_t d = -1, gn = 0;
+            if (mode == MODE_LP && active && bq >= 0) {
+                const int64_t gg = (int64_t)bk - own;
+                if (lp_candidate(gg, own, den)) {
+                    d = bq; gn = (int32_t)gg;
+                    atomicAdd((unsigned long long*)&status[S_CDEG], (unsigned long long)(end - beg));
+                }
+            } else if (mode == MODE_RB && active) {
+                const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
+                d = bq >= 0 ? bq : light;
+                const int32_t loss = (int32_t)(own - cd);
+                gn = -loss;
+                unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NCAND], 1ull);
+                ckeys[slot] = ((uint64_t)p << 41) | ((uint64_t)loss_bucket(loss) << 31) | (uint64_t)v;
+                cvals[slot] = (int32_t)v;
+            }
+            dest[v] = d; gain[v] = gn;
+        }
+    } else {
+        // ---- one row per warp
+        int32_t* hist = hist_all + w * k;
+        const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - nheavy) * RT) >> 5;
+        for (int64_t v = wid; v < g.n; v += nw) {
+            const int64_t beg = g.rp[v], end = g.rp[v + 1];
+            if (end - beg > kHeavyDeg) continue;
+            const int32_t p = part[v];
+            const bool active = (mode == MODE_LP && !lock[v]) || (mode == MODE_RB && over[p]);
+            int32_t cross = 0, tot = 0;
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const int32_t q = part[g.ci[e]];
+                const int32_t wt = g.ew ? g.ew[e] : 1;
+                tot += wt;
+                if (q != p) cross += wt;
+                if (active) atomicAdd(&hist[q], wt);
+            }
+            cross = warp_sum(cross); tot = warp_sum(tot);
+            if (lane == 0) acc += cross;
+            if (!active) {
+                if (lane == 0) { dest[v] = -1; gain[v] = 0; }
+                continue;
+            }
+            __syncwarp();
+            uint64_t bk = 0; int32_t bq = -1;
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const int32_t q = part[g.ci[e]];
+                if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+            }
+            warp_argmax_q(bk, bq);
+            __syncwarp();
+            for (int64_t e = beg + lane; e < end; e += 32) hist[part[g.ci[e]]] = 0;
+            __syncwarp();
+            if (lane == 0) {
+                const int64_t own = tot - cross;
+                int32_t d = -1, gn = 0;
+                if (mode == MODE_LP) {
+                    if (bq >= 0) {
+                        const int64_t gg = (int64_t)bk - own;
+                        if (lp_candidate(gg, own, den)) {
+                            d = bq; gn = (int32_t)gg;
+                            unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NLIST], 1ull);
+                            clist[slot] = (int32_t)v;
+                            atomicAdd((unsigned long long*)&status[S_CDEG], (unsigned long long)(end - beg));
+                        }
+                    }
+                } else {
+                    const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
+                    d = bq >= 0 ? bq : light;
+                    const int32_t loss = (int32_t)(own - cd);
+                    gn = -loss;
+                    unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NCAND], 1ull);
+                    ckeys[slot] = ((uint64_t)p << 41) | ((uint64_t)loss_bucket(loss) << 31) | (uint64_t)v;
+                    cvals[slot] = (int32_t)v;
+                }
+                dest[v] = d; gain[v] = gn;
+            }
+        }
+    }
+    acc = warp_sum(acc);
+    __syncthreads();
+    if (lane == 0) s_red[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t s = 0;
+        for (int i = 0; i < RW; ++i) s += s_red[i];
+        if (s) atomicAdd((unsigned long long*)&status[S_CROSS], (unsigned long long)s);
+    }
+}
+
+// ------------------------------------------------------------------ LP apply
+__global__ void k_copy_state(int64_t n, const int32_t* __restrict__ part, int32_t* __restrict__ part_next,
+                             uint8_t* __restrict__ lock_next) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        part_next[v] = part[v];
+        lock_next[v] = 0;
+    }
+}
+
+__device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v, int32_t p, int32_t d, int32_t gv,
+                                           const int32_t* __restrict__ part, const int32_t* __restrict__ dest,
+                                           const int32_t* __restrict__ gain) {
+    const int32_t u = g.ci[e];
+    int32_t pu = part[u];
+    const int32_t du = dest[u];
+    if (du >= 0) {
+        const int32_t gu = gain[u];
+        if (gu > gv || (gu == gv && u < (int32_t)v)) pu = du;
+    }
+    const int32_t wt = g.ew ? g.ew[e] : 1;
+    return pu == d ? wt : (pu == p ? -wt : 0);
+}
+
+__global__ void __launch_bounds__(RT) k_lp_apply(DGraph g, int32_t k, const int32_t* __restrict__ part,
+                                                 const int32_t* __restrict__ dest, const int32_t* __restrict__ gain,
+                                                 const int32_t* __restrict__ heavy, int64_t nheavy,
+                                                 const int32_t* __restrict__ clist, const int64_t* __restrict__ status,
+                                                 int32_t* __restrict__ part_next, uint8_t* __restrict__ lock_next,
+                                                 int64_t* __restrict__ pw, int64_t* __restrict__ moves_out) {
+    extern __shared__ int64_t delta[];
+    __shared__ int32_t s_red[RW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = threadIdx.x; q < k; q += RT) delta[q] = 0;
+    __syncthreads();
+    int64_t moves = 0;
+    if ((int64_t)blockIdx.x < nheavy) {
+        const int64_t v = heavy[blockIdx.x];
+        const int32_t d = dest[v];
+        if (d >= 0) {
+            const int32_t p = part[v], gv = gain[v];
+            int32_t g2 = 0;
+            for (int64_t e = g.rp[v] + threadIdx.x; e < g.rp[v + 1]; e += RT) g2 += ab_term(g, e, v, p, d, gv, part, dest, gain);
+            g2 = warp_sum(g2);
+            if (lane == 0) s_red[w] = g2;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int32_t s = 0;
+                for (int i = 0; i < RW; ++i) s += s_red[i];
+                if (s >= 0) {
+                    part_next[v] = d; lock_next[v] = 1;
+                    const int64_t wv = g.vw ? g.vw[v] : 1;
+                    atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
+                    atomicAdd((unsigned long long*)&delta[p], (unsigned long long)(-wv));
+                    moves = 1;
+                }
+            }
+        }
+    } else {
+        const int64_t ncl = status[S_NLIST];
+        const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - nheavy) * RT) >> 5;
+        for (int64_t i = wid; i < ncl; i += nw) {
+            const int64_t v = clist[i];
+            const int32_t d = dest[v], p = part[v], gv = gain[v];
+            int32_t g2 = 0;
+            for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32) g2 += ab_term(g, e, v, p, d, gv, part, dest, gain);
+            g2 = warp_sum(g2);
+            if (lane == 0 && g2 >= 0) {
+                part_next[v] = d; lock_next[v] = 1;
+                const int64_t wv = g.vw ? g.vw[v] : 1;
+                atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
+                atomicAdd((unsigned long long*)&delta[p], (unsigned long long)(-wv));
+                ++moves;
+            }
+        }
+    }
+    moves = warp_sum(moves);
+    __syncthreads();
+    if (lane == 0 && moves) atomicAdd((unsigned long long*)moves_out, (unsigned long long)moves);
+    for (int q = threadIdx.x; q < k; q += RT)
+        if (delta[q]) atomicAdd((unsigned long long*)&pw[q], (unsigned long long)delta[q]);
+}
+
+// ------------------------------------------------------------------ rebalance
+__global__ void k_gather_vw(int64_t cnt, const int32_t* __restrict__ vidx, const int32_t* __restrict__ vw,
+                            int32_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = vw ? vw[vidx[i]] : 1;
+}
+
+__device__ __forceinline__ int64_t seg_start(const uint64_t* keys, int64_t i, uint64_t seg) {
+    int64_t lo = 0, hi = i;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if ((keys[mid] >> 41) < seg) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// flag[i] = 1 when the move keeps its source within the excess prefix
+__global__ void k_rb_source(int64_t cnt, const uint64_t* __restrict__ keys, const int64_t* __restrict__ pre,
+                            const int64_t* __restrict__ pw, int64_t Lmax, int32_t* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t src = keys[i] >> 41;
+        const int64_t s = seg_start(keys, i, src);
+        flag[i] = (pre[i] - pre[s]) < (pw[src] - Lmax) ? 1 : 0;
+    }
+}
+
+// weak: re-key accepted moves by destination
+__global__ void k_rb_rekey(int64_t cnt, const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals,
+                           const int32_t* __restrict__ flag, const int32_t* __restrict__ dest,
+                           uint64_t* __restrict__ keys2, int32_t* __restrict__ vals2, int64_t* __restrict__ cnt2) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!flag[i]) continue;
+        const int32_t v = vals[i];
+        const uint64_t low = keys[i] & ((1ull << 41) - 1);  // bucket | id
+        unsigned long long slot = atomicAdd((unsigned long long*)cnt2, 1ull);
+        keys2[slot] = ((uint64_t)(uint32_t)dest[v] << 41) | low;
+        vals2[slot] = v;
+    }
+}
+
+// weak: keep moves whose destination prefix fits the capacity; apply
+__global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals,
+                                const int64_t* __restrict__ pre, const int32_t* __restrict__ vw,
+                                const int64_t* __restrict__ pw_snap, int64_t Lmax, int32_t* __restrict__ part,
+                                uint8_t* __restrict__ lock, int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t d = keys[i] >> 41;
+        const int64_t s = seg_start(keys, i, d);
+        const int32_t v = vals[i];
+        const int64_t wv = vw ? vw[v] : 1;
+        if ((pre[i] - pre[s]) + wv <= Lmax - pw_snap[d]) {
+            const int32_t p = part[v];
+            part[v] = (int32_t)d; lock[v] = 1;
+            atomicAdd((unsigned long long*)&pw[d], (unsigned long long)wv);
+            atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
+            atomicAdd((unsigned long long*)moves, 1ull);
+        }
+    }
+}
+
+// strong: cumulative free capacity of non-overweight parts
+__global__ void k_cumfree(int32_t k, const int64_t* __restrict__ pw, int64_t Lmax, int64_t* __restrict__ cum) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int64_t s = 0;
+    cum[0] = 0;
+    for (int q = 0; q < k; ++q) {
+        const int64_t x = pw[q];
+        s += (x > Lmax) ? 0 : (Lmax - x);
+        cum[q + 1] = s;
+    }
+}
+
+__global__ void k_mask_vw(int64_t cnt, const int32_t* __restrict__ flag, const int32_t* __restrict__ wvals,
+                          int32_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = flag[i] ? wvals[i] : 0;
+}
+
+__global__ void k_rb_strong_apply(int64_t cnt, const int32_t* __restrict__ vals, const int32_t* __restrict__ flag,
+                                  const int64_t* __restrict__ P, const int32_t* __restrict__ vw,
+                                  const int64_t* __restrict__ cum, int32_t k, int32_t* __restrict__ part,
+                                  uint8_t* __restrict__ lock, int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        if (!flag[i]) continue;
+        const int64_t pre = P[i];
+        if (pre >= cum[k]) continue;
+        // q with cum[q] <= pre < cum[q+1]: last index with cum <= pre
+        int lo = 0, hi = k;  // search in cum[0..k]
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (cum[mid] <= pre) lo = mid; else hi = mid - 1;
+        }
+        const int q = lo;
+        const int32_t v = vals[i];
+        const int64_t wv = vw ? vw[v] : 1;
+        if (q < k && pre + wv <= cum[q + 1]) {
+            const int32_t p = part[v];
+            part[v] = q; lock[v] = 1;
+            atomicAdd((unsigned long long*)&pw[q], (unsigned long long)wv);
+            atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
+            atomicAdd((unsigned long long*)moves, 1ull);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ projection, weights, cut
+__global__ void k_project(int64_t n, const int32_t* __restrict__ cmap, const int32_t* __restrict__ pc,
+                          int32_t* __restrict__ pf) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        pf[v] = pc[cmap[v]];
+}
+
+__global__ void k_part_weights(int64_t n, const int32_t* __restrict__ part, const int32_t* __restrict__ vw, int32_t k,
+                               int64_t* __restrict__ pw) {
+    extern __shared__ int64_t spw[];
+    for (int q = threadIdx.x; q < k; q += blockDim.x) spw[q] = 0;
+    __syncthreads();
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd((unsigned long long*)&spw[part[v]], (unsigned long long)(vw ? vw[v] : 1));
+    __syncthreads();
+    for (int q = threadIdx.x; q < k; q += blockDim.x)
+        if (spw[q]) atomicAdd((unsigned long long*)&pw[q], (unsigned long long)spw[q]);
+}
+
+// warp per row: directed cross weight (d_cross2 accumulates 2*cut)
+__global__ void __launch_bounds__(RT) k_cut(DGraph g, const int32_t* __restrict__ part, int64_t* __restrict__ cross2) {
+    __shared__ int64_t s_red[RW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t wid = ((int64_t)blockIdx.x * RT + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * RT) >> 5;
+    int64_t acc = 0;
+    for (int64_t v = wid; v < g.n; v += nw) {
+        const int32_t p = part[v];
+        for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32)
+            if (part[g.ci[e]] != p) acc += g.ew ? g.ew[e] : 1;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) s_red[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t s = 0;
+        for (int i = 0; i < RW; ++i) s += s_red[i];
+        if (s) atomicAdd((unsigned long long*)cross2, (unsigned long long)s);
+    }
+}
+
+void project(Ctx& c, const Level& fine, const int32_t* part_coarse, int32_t* part_fine) {
+    k_project<<<grid_for(fine.g.n, 256), 256, 0, c.s>>>(fine.g.n, fine.cmap, part_coarse, part_fine);
+    GP_LAUNCHED(c);
+    c.bytes += 12 * fine.g.n;
+}
+
+void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* pw) {
+    memset_async(c, pw, 0, sizeof(int64_t) * k);
+    k_part_weights<<<grid_for(g.n, 256, c.sm_count * 4), 256, sizeof(int64_t) * k, c.s>>>(g.n, part, g.vw, k, pw);
+    GP_LAUNCHED(c);
+    c.bytes += 4 * g.n + (g.vw ? 4 * g.n : 0);
+}
+
+void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw) {
+    memset_async(c, d_cross2, 0, sizeof(int64_t));
+    k_cut<<<grid_for(g.n * 32, RT, c.sm_count * 8), RT, 0, c.s>>>(g, part, d_cross2);
+    GP_LAUNCHED(c);
+    c.bytes += 8 * (g.n + 1) + 8 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.n;
+    if (d_pw) part_weights(c, g, part, k, d_pw);
+}
+
+// ------------------------------------------------------------------ level controller
+static int bits_for(int64_t x) {
+    int b = 1;
+    while ((1ll << b) < x) ++b;
+    return b;
+}
+
+static void trace_iter(Ctx& c, const RefineBufs& B, int64_t n, int64_t m, int level, int it, int mode,
+                       int64_t cut_before, int64_t mp_before, const Tracer& tr) {
+    std::vector<int32_t> d(n), gn(n), p(n);
+    GP_CUDA(cudaMemcpyAsync(d.data(), B.dest, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(gn.data(), B.gain, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(p.data(), B.part, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, B.status + S_STEP_MOVES, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    c.sync();
+    gp_trace_event ev;
+    memset(&ev, 0, sizeof ev);
+    ev.kind = GP_TR_REFINE_ITER; ev.level = level; ev.iter = it; ev.mode = mode;
+    ev.n = n; ev.m = m; ev.cut = cut_before; ev.maxpw = mp_before; ev.count = c.h_pinned[0];
+    ev.a0 = d.data(); ev.a1 = gn.data(); ev.a2 = p.data();
+    tr.emit(ev);
+}
+
+int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr) {
+    const DGraph& g = L.g;
+    const int64_t n = g.n;
+    const int32_t k = P.k;
+    const int64_t Lmax = P.Lmax;
+    memset_async(c, B.lock, 0, n);
+    const int kpad = (k + 15) & ~15;
+    const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
+    GP_CUDA(cudaFuncSetAttribute(k_conn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conn_smem));
+    const int light_blocks = grid_for(n * 32, RT, c.sm_count * 8);
+    const int grid = (int)L.nheavy + light_blocks;
+    int64_t best_cut = 0, best_mp = 0;
+    int stall = 0, rb_streak = 0, steps = 0, last_mode = MODE_LP;
+    int64_t prev_moves = -1;
+    const int nb_k = bits_for(k);
+    for (int it = 0;; ++it) {
+        const bool final_eval = (it == P.o.refine_max_iters);
+        GP_CUDA(cudaMemsetAsync(B.status, 0, sizeof(int64_t) * S_NRESET, c.s));
+        k_conn<<<grid, RT, conn_smem, c.s>>>(g, k, Lmax, P.o.lp_filter_den, final_eval ? 1 : 0, B.part, B.lock, B.pw,
+                                             L.heavy, L.nheavy, B.dest, B.gain, B.status, B.ckeys, B.cvals, B.clist);
+        GP_LAUNCHED(c);
+        c.bytes += L.scan_bytes() + 4 * n + n + 8 * n;
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned, B.status, sizeof(int64_t) * S_NSLOTS, cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        const int64_t cur_cut = c.h_pinned[S_CROSS] / 2;
+        const int64_t cur_mp = c.h_pinned[S_MAXPW];
+        const int dev_mode = (int)c.h_pinned[S_MODE];
+        const int64_t ncand = c.h_pinned[S_NCAND];
+        const int64_t nlist = c.h_pinned[S_NLIST];
+        const int64_t cdeg = c.h_pinned[S_CDEG];
+        if (it == 0) {
+            best_cut = cur_cut; best_mp = cur_mp;
+            GP_CUDA(cudaMemcpyAsync(B.best, B.part, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c.s));
+            GP_CUDA(cudaMemcpyAsync(B.best_pw, B.pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
+        } else {
+            const int64_t nmoves = c.h_pinned[S_STEP_MOVES];
+            const bool cb = cur_mp <= Lmax, bb = best_mp <= Lmax;
+            bool better = false, signif = false;
+            if (cb && !bb) { better = true; signif = true; }
+            else if (cb && bb) { better = cur_cut < best_cut; signif = 1000 * cur_cut < 999 * best_cut; }
+            else if (!cb && !bb) { better = cur_mp < best_mp || (cur_mp == best_mp && cur_cut < best_cut); signif = cur_mp < best_mp; }
+            if (better) {
+                best_cut = cur_cut; best_mp = cur_mp;
+                GP_CUDA(cudaMemcpyAsync(B.best, B.part, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c.s));
+                GP_CUDA(cudaMemcpyAsync(B.best_pw, B.pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
+            }
+            stall = signif ? 0 : stall + 1;
+            const bool lp_idle = (last_mode == MODE_LP && nmoves == 0 && prev_moves == 0);
+            prev_moves = nmoves;
+            if (stall >= P.o.refine_patience || lp_idle) break;
+        }
+        if (final_eval) break;
+        int mode;
+        if (dev_mode == MODE_RB) { mode = (rb_streak >= P.o.strong_after) ? 2 : 1; ++rb_streak; }
+        else { mode = 0; rb_streak = 0; }
+        last_mode = (mode == 0) ? MODE_LP : MODE_RB;
+        int64_t* moves_d = B.status + S_STEP_MOVES;  // moves of this step, read at the next sync
+        memset_async(c, moves_d, 0, sizeof(int64_t));
+        if (mode == 0) {
+            k_copy_state<<<grid_for(n, 256), 256, 0, c.s>>>(n, B.part, B.part_next, B.lock_next);
+            GP_LAUNCHED(c);
+            k_lp_apply<<<grid, RT, sizeof(int64_t) * k, c.s>>>(g, k, B.part, B.dest, B.gain, L.heavy, L.nheavy, B.clist,
+                                                              B.status, B.part_next, B.lock_next, B.pw, moves_d);
+            GP_LAUNCHED(c);
+            // copy pass + afterburner: candidate rows with three gathered int32 per entry
+            c.bytes += 9 * n + 16 * nlist + cdeg * (4 + (g.ew ? 4 : 0) + 12);
+            std::swap(B.part, B.part_next);
+            std::swap(B.lock, B.lock_next);
+        } else {
+            memset_async(c, B.lock, 0, n);
+            if (ncand > 0) {
+                auto mk = c.tmp->save();
+                const int bits = 41 + nb_k;
+                radix_sort_pairs(c, B.ckeys, B.cvals, B.ckeys2, B.cvals2, ncand, bits);
+                int32_t* wv = c.tmp_alloc<int32_t>(ncand);
+                int64_t* pre = c.tmp_alloc<int64_t>(ncand);
+                int32_t* flag = c.tmp_alloc<int32_t>(ncand);
+                int64_t* pw_snap = c.tmp_alloc<int64_t>(k);
+                GP_CUDA(cudaMemcpyAsync(pw_snap, B.pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
+                k_gather_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, g.vw, wv);
+                GP_LAUNCHED(c);
+                scan_excl_i32_to_i64(c, wv, pre, ncand, nullptr);
+                k_rb_source<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, pre, B.pw, Lmax, flag);
+                GP_LAUNCHED(c);
+                if (mode == 1) {
+                    int64_t* cnt2 = c.tmp_alloc<int64_t>(1);
+                    memset_async(c, cnt2, 0, sizeof(int64_t));
+                    k_rb_rekey<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, B.cvals, flag, B.dest,
+                                                                    B.ckeys2, B.cvals2, cnt2);
+                    GP_LAUNCHED(c);
+                    const int64_t n2 = read_i64(c, cnt2);
+                    if (n2 > 0) {
+                        radix_sort_pairs(c, B.ckeys2, B.cvals2, B.ckeys, B.cvals, n2, bits);
+                        k_gather_vw<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.cvals2, g.vw, wv);
+                        GP_LAUNCHED(c);
+                        scan_excl_i32_to_i64(c, wv, pre, n2, nullptr);
+                        k_rb_weak_apply<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.ckeys2, B.cvals2, pre, g.vw, pw_snap,
+                                                                           Lmax, B.part, B.lock, B.pw, moves_d);
+                        GP_LAUNCHED(c);
+                    }
+                } else {
+                    int64_t* cum = c.tmp_alloc<int64_t>(k + 1);
+                    int32_t* wm = c.tmp_alloc<int32_t>(ncand);
+                    k_cumfree<<<1, 32, 0, c.s>>>(k, B.pw, Lmax, cum);
+                    GP_LAUNCHED(c);
+                    k_mask_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, flag, wv, wm);
+                    GP_LAUNCHED(c);
+                    scan_excl_i32_to_i64(c, wm, pre, ncand, nullptr);
+                    k_rb_strong_apply<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, flag, pre, g.vw, cum, k,
+                                                                           B.part, B.lock, B.pw, moves_d);
+                    GP_LAUNCHED(c);
+                }
+                c.bytes += 60 * ncand;
+                c.tmp->restore(mk);
+            }
+        }
+        ++steps;
+        if (tr.on()) trace_iter(c, B, n, g.m, level, it, mode, cur_cut, cur_mp, tr);
+    }
+    GP_CUDA(cudaMemcpyAsync(B.part, B.best, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c.s));
+    GP_CUDA(cudaMemcpyAsync(B.pw, B.best_pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
+    return steps;
+}
+
+}  // namespace gp
