@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark: edges/sec partitioned at k=64 on one B200.
+
+Workload: R-MAT scale 24, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05),
+deduplicated, symmetrized, isolated vertices removed (~16.7M vertices, ~250M
+undirected edges), int64 row pointers / int32 column ids, unit weights,
+k = 64, imbalance 3%, seed 0.  The graph is generated on the device from a
+counter-based hash (synthetic stand-in; no dataset is read).
+
+A step is one full V-cycle (gp_partition_device) over the resident graph.
+value  = undirected edges x steps x ranks / max-over-ranks device time.
+e2e    = the same metric through the host entry point gp_partition with the
+         graph in pinned host memory: host->device copy of the CSR and
+         device->host copy of the part array inside every step.
+Multi-GPU: one independent replica per rank (a single graph does not shard).
+
+--impl reference runs the CPU oracle (the sequential restatement of the same
+rules; the reference has no CPU implementation of this path) on a bounded
+R-MAT sample on rank 0 and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edges/sec partitioned at k=64 on 1 B200; exact cut+imbalance vs plain & METIS"
+REASON_BITS = {
+    0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+    0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+    0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--k", type=int, default=64)
+    ap.add_argument("--imbalance", type=float, default=0.03)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--sample-scale", type=int, default=17, help="R-MAT scale of the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--metis-full", action="store_true", help="also run METIS on the full workload (minutes)")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,utilization.gpu"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 5:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        for r in self.rows:
+            try:
+                clk, mx, util = float(r[0]), float(r[1]), float(r[4])
+                bits = int(r[3], 16)
+            except ValueError:
+                continue
+            smax.append(mx)
+            if util > 0:
+                sm.append(clk)
+            for b, name in REASON_BITS.items():
+                if bits & b and name != "gpu_idle":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(workload_key):
+    """DRAM bytes per connectivity-pass launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload_key)
+    except (OSError, ValueError):
+        return None
+
+
+def make_graph(scale, seed, device):
+    from thegraphpartitioning_b200 import graphs
+    rp, ci, n_all = graphs.rmat(scale, 16, seed=seed, device=device)
+    return rp, ci, n_all
+
+
+def cpu_sample(args):
+    """Oracle, METIS and the GPU on the same bounded R-MAT sample."""
+    import numpy as np
+    import oracle
+    import thegraphpartitioning_b200 as gp
+    oracle.build()
+    rp, ci, _ = make_graph(args.sample_scale, args.seed, "cpu")
+    rp_np, ci_np = rp.numpy(), ci.numpy()
+    m = len(ci_np) // 2
+    t = time.perf_counter()
+    part, st, _ = oracle.partition(rp_np, ci_np, args.k, args.imbalance, args.seed)
+    t_oracle = time.perf_counter() - t
+    mpart, mcut, t_metis = oracle.metis(rp_np, ci_np, args.k, seed=args.seed)
+    _, mpw = oracle.edge_cut(rp_np, ci_np, mpart, args.k)
+    gpart, gst, _ = gp.partition(rp.cuda(), ci.cuda(), args.k, args.imbalance, args.seed)
+    same = bool(np.array_equal(gpart.cpu().numpy(), part))
+    total = len(rp_np) - 1
+    sample = f"R-MAT scale {args.sample_scale} EF16 ({total} vertices, {m} undirected edges), k={args.k}, full V-cycle"
+    return {
+        "cpu_baseline": {"value": m / t_oracle, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample,
+                         "seconds": t_oracle},
+        "quality_sample": {"sample": sample, "gpu_cut": gst["cut"], "gpu_imbalance": round(gst["imbalance"], 5),
+                           "oracle_cut": st["cut"], "gpu_equals_oracle": same,
+                           "metis_cut": mcut, "metis_imbalance": round(float(mpw.max()) * args.k / total - 1, 5),
+                           "metis_seconds": t_metis, "metis_cores": 1,
+                           "cut_vs_metis": round(gst["cut"] / max(mcut, 1), 4)},
+    }
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    rp, ci, _ = make_graph(args.sample_scale, args.seed, "cpu")
+    rp_np, ci_np = rp.numpy(), ci.numpy()
+    m = len(ci_np) // 2
+    for _ in range(args.warmup):
+        oracle.partition(rp_np, ci_np, args.k, args.imbalance, args.seed)
+    times = []
+    cut = None
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        _, st, _ = oracle.partition(rp_np, ci_np, args.k, args.imbalance, args.seed)
+        times.append(time.perf_counter() - t)
+        cut = st["cut"]
+    tot = sum(times)
+    value = m * args.steps / tot
+    sample = f"R-MAT scale {args.sample_scale} EF16 ({len(rp_np) - 1} vertices, {m} undirected edges), k={args.k}"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT sample)",
+        "config": {"workload": f"rmat{args.scale}_ef16_k{args.k}", "k": args.k, "imbalance": args.imbalance,
+                   "seed": args.seed, "timed_sample": sample, "cut": cut},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's path runs only on a GPU with an external gpmetis; its CPU counterpart "
+                "here is the oracle (sequential restatement of the same deterministic rules, 1 core)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import thegraphpartitioning_b200 as gp
+    from thegraphpartitioning_b200._abi import make_options
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    gp.lib()
+    rp, ci, n_all = make_graph(args.scale, args.seed, dev)
+    n = rp.numel() - 1
+    m = ci.numel() // 2
+    torch.cuda.synchronize()
+    opts = make_options(profile=1)
+    stream = torch.cuda.current_stream(dev)
+    part = torch.empty(n, dtype=torch.int32, device=dev)
+    for _ in range(args.warmup):
+        gp.partition(rp, ci, args.k, args.imbalance, args.seed, options=opts, out=part)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stats = []
+    with ClockSampler(local) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            _, st, _ = gp.partition(rp, ci, args.k, args.imbalance, args.seed, options=opts, out=part)
+            stats.append(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+        dist.barrier()
+    value = m * args.steps * world / (t_ms / 1e3)
+    ms_conn = sum(s["ms_conn"] for s in stats)
+    conn_launches = sum(s["conn_launches"] for s in stats)
+    conn_bytes = sum(s["conn_bytes"] for s in stats)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = (conn_bytes / (ms_conn / 1e3)) / 1e9 if ms_conn > 0 else None
+    wl = f"rmat{args.scale}_ef16_k{args.k}"
+    traffic = traffic_per_launch(wl)
+    last = stats[-1]
+
+    # end to end through the host entry point with pinned host buffers
+    rp_h = rp.cpu().pin_memory()
+    ci_h = ci.cpu().pin_memory()
+    out_h = torch.empty(n, dtype=torch.int32).pin_memory()
+    import ctypes as C
+    L = gp.lib()
+    from thegraphpartitioning_b200._abi import GpStats
+    P64, P32 = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+    est = GpStats()
+    def host_call():
+        rc = L.gp_partition_ex(n, C.cast(rp_h.data_ptr(), P64), C.cast(ci_h.data_ptr(), P32), None, None, args.k,
+                               args.imbalance, args.seed, C.cast(out_h.data_ptr(), P32), C.byref(opts), C.byref(est),
+                               None, None)
+        if rc != 0:
+            raise RuntimeError(L.gp_last_error().decode())
+    host_call()  # warm
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        host_call()
+    t_e2e = time.perf_counter() - t
+    if dist:
+        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e_value = m * args.e2e_steps * world / t_e2e
+    assert torch.equal(out_h, part.cpu()), "host and device entry points disagree"
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT generated on device)",
+            "config": {"workload": wl, "scale": args.scale, "edge_factor": 16, "n": n, "n_before_isolated": n_all,
+                       "m_undirected": m, "k": args.k, "imbalance": args.imbalance, "seed": args.seed,
+                       "index_types": "int64 rowptr / int32 colidx", "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (CSR %.1f GB)" % ((8 * (n + 1) + 8 * m) / 1e9)},
+            "result": {"cut": last["cut"], "imbalance": round(last["imbalance"], 5),
+                       "max_part_weight": last["max_part_weight"], "max_allowed": last["max_allowed"],
+                       "levels": last["levels"], "coarsest_n": last["coarsest_n"],
+                       "refine_iters": last["refine_iters"],
+                       "ms_coarsen": last["ms_coarsen"], "ms_initial": last["ms_initial"],
+                       "ms_refine": last["ms_refine"], "algo_bytes_per_step": last["algo_bytes"]},
+            "roofline": {"bound": "hbm", "kernel": "k_conn (refinement connectivity pass)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic, "launches": conn_launches,
+                         "avg_launch_ms": ms_conn / max(conn_launches, 1),
+                         "algo_bytes_per_launch": conn_bytes / max(conn_launches, 1),
+                         "share_of_step": ms_conn / t_ms},
+            "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": 8 * (n + 1) + 4 * 2 * m,
+                    "d2h_bytes_per_step": 4 * n, "ms_per_step": 1e3 * t_e2e / args.e2e_steps},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line.update(cpu_sample(args))
+        if args.metis_full:
+            import oracle
+            mpart, mcut, t_metis = oracle.metis(rp.cpu().numpy(), ci.cpu().numpy(), args.k, seed=args.seed)
+            line["metis_full"] = {"cut": mcut, "seconds": t_metis, "cores": 1,
+                                  "cut_ratio": last["cut"] / max(mcut, 1),
+                                  "speedup_vs_metis": t_metis / (t_ms / 1e3 / args.steps)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

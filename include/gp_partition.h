@@ -66,7 +66,8 @@ typedef struct gp_options {
     int32_t strong_after;       /* consecutive rebalance iterations before strong (2)  */
     int32_t check_input;        /* 0/1: structural checks, 2: +symmetry, <0: none        */
     int32_t verbose;            /* 0: silent                                           */
-    int32_t reserved[5];
+    int32_t profile;            /* 1: time the connectivity pass with CUDA events       */
+    int32_t reserved[4];
 } gp_options;
 
 /* Result record of one call. */
@@ -89,6 +90,10 @@ typedef struct gp_stats {
     double  ms_total;
     double  ms_h2d;             /* host API only: host->device copies                  */
     double  ms_d2h;
+    /* opt.profile = 1: the refinement connectivity pass (the dominant kernel) */
+    double  ms_conn;            /* summed CUDA-event time of its launches               */
+    int64_t conn_launches;
+    int64_t conn_bytes;         /* algorithmic bytes of those launches                 */
 } gp_stats;
 
 /* ---- optional tracing (tests): host copies of intermediate results ----- */

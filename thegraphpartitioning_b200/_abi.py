@@ -46,7 +46,8 @@ class GpOptions(C.Structure):
         ("strong_after", C.c_int32),
         ("check_input", C.c_int32),
         ("verbose", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("profile", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -70,6 +71,9 @@ class GpStats(C.Structure):
         ("ms_total", C.c_double),
         ("ms_h2d", C.c_double),
         ("ms_d2h", C.c_double),
+        ("ms_conn", C.c_double),
+        ("conn_launches", C.c_int64),
+        ("conn_bytes", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

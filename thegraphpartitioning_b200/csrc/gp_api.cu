@@ -212,6 +212,8 @@ static void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uin
     resolve_options(opt, k, &P.o);
     P.k = k; P.seed = seed; P.imbalance = imbalance;
     Timer tm;
+    c.profile = P.o.profile > 0;
+    if (c.profile) { c.ev_a = tm.e[6]; c.ev_b = tm.e[7]; }
     GP_CUDA(cudaEventRecord(tm.e[0], c.s));
     P.W = validate(c, g0, P.o.check_input);
     P.Lmax = compute_lmax(P.W, k, imbalance);
@@ -341,6 +343,9 @@ static void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uin
         st->ms_initial = ms_init;
         st->ms_refine = ms_refine;
         st->ms_total = tm.ms(0, 3);
+        st->ms_conn = c.ms_conn;
+        st->conn_launches = c.conn_launches;
+        st->conn_bytes = c.conn_bytes;
     }
 }
 

@@ -110,6 +110,11 @@ struct Ctx {
     int64_t bytes = 0;         // algorithmic bytes of executed passes
     int sm_count = 148;
     int64_t* h_pinned = nullptr;  // small pinned staging buffer (64 int64)
+    // opt-in timing of the connectivity pass
+    bool profile = false;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    double ms_conn = 0;
+    int64_t conn_launches = 0, conn_bytes = 0;
     template <class T> T* keep_alloc(int64_t count) { return (T*)keep->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
     template <class T> T* tmp_alloc(int64_t count) { return (T*)tmp->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
     void sync() { GP_CUDA(cudaStreamSynchronize(s)); }

@@ -522,12 +522,23 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     for (int it = 0;; ++it) {
         const bool final_eval = (it == P.o.refine_max_iters);
         GP_CUDA(cudaMemsetAsync(B.status, 0, sizeof(int64_t) * S_NRESET, c.s));
+        if (c.profile) GP_CUDA(cudaEventRecord(c.ev_a, c.s));
         k_conn<<<grid, RT, conn_smem, c.s>>>(g, k, Lmax, P.o.lp_filter_den, final_eval ? 1 : 0, B.part, B.lock, B.pw,
                                              L.heavy, L.nheavy, B.dest, B.gain, B.status, B.ckeys, B.cvals, B.clist);
         GP_LAUNCHED(c);
-        c.bytes += L.scan_bytes() + 4 * n + n + 8 * n;
+        if (c.profile) GP_CUDA(cudaEventRecord(c.ev_b, c.s));
+        // rowptr, colidx, weights, gathered part[u]; part[v], lock[v] read; dest, gain written
+        const int64_t conn_bytes = L.scan_bytes() + 4 * n + n + 8 * n;
+        c.bytes += conn_bytes;
         GP_CUDA(cudaMemcpyAsync(c.h_pinned, B.status, sizeof(int64_t) * S_NSLOTS, cudaMemcpyDeviceToHost, c.s));
         c.sync();
+        if (c.profile) {
+            float t = 0;
+            GP_CUDA(cudaEventElapsedTime(&t, c.ev_a, c.ev_b));
+            c.ms_conn += t;
+            c.conn_launches += 1;
+            c.conn_bytes += conn_bytes;
+        }
         const int64_t cur_cut = c.h_pinned[S_CROSS] / 2;
         const int64_t cur_mp = c.h_pinned[S_MAXPW];
         const int dev_mode = (int)c.h_pinned[S_MODE];
