@@ -54,6 +54,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--metis-full", action="store_true", help="also run METIS on the full workload (minutes)")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="one warm partition, then exactly one partition between cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off); prints nothing else")
     return ap.parse_args()
 
 
@@ -226,6 +229,16 @@ def main():
     opts = make_options(profile=1)
     stream = torch.cuda.current_stream(dev)
     part = torch.empty(n, dtype=torch.int32, device=dev)
+    if args.profile_once:
+        gp.partition(rp, ci, args.k, args.imbalance, args.seed, out=part)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        _, st, _ = gp.partition(rp, ci, args.k, args.imbalance, args.seed, out=part)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_once": f"rmat{args.scale}_ef16_k{args.k}", "n": n, "m": m,
+                          "launches": st["kernel_launches"], "cut": st["cut"]}), flush=True)
+        return
     for _ in range(args.warmup):
         gp.partition(rp, ci, args.k, args.imbalance, args.seed, options=opts, out=part)
     torch.cuda.synchronize()
