@@ -223,9 +223,11 @@ std::vector<int32_t> match_level(const Graph& g, int level, const Params& P, int
 // prefix_sum + fillEdgeArrays (src/gpu_part.cu:109-242): the coarse vertex of
 // a pair {a<b} is represented by a; coarse ids are an exclusive scan of the
 // representative flags in vertex order (not an atomic counter); the coarse
-// row of c is N(a) u N(b) mapped through cmap, without c itself, sorted by
-// coarse id, duplicates merged with summed weights (not a 64-bit mod mask);
-// coarse vertex weight = sum of the fine weights (the reference keeps none).
+// row of c lists the coarse neighbours met while walking N(a) then N(b) in
+// CSR order, mapped through cmap, without c itself, each at the position of
+// its first occurrence, with the weights of all its occurrences summed (not
+// a 64-bit mod mask that drops colliding neighbours); coarse vertex weight =
+// sum of the fine weights (the reference keeps none).
 void contract(const Graph& g, const std::vector<int32_t>& match, std::vector<int32_t>& cmap, Graph& cg) {
     const int64_t n = g.n;
     cmap.assign(n, -1);
@@ -243,9 +245,8 @@ void contract(const Graph& g, const std::vector<int32_t>& match, std::vector<int
     cg.rp.assign(nc + 1, 0);
     cg.vw.assign(nc, 0);
     cg.ci.clear(); cg.ew.clear();
-    std::vector<std::pair<int32_t, int32_t>> row;
+    std::vector<int64_t> stamp(nc, -1), slot(nc, 0);
     for (int64_t c = 0; c < nc; ++c) {
-        row.clear();
         int32_t mem[2] = {first[c], second[c]};
         int64_t vwsum = 0;
         for (int t = 0; t < 2; ++t) {
@@ -253,21 +254,19 @@ void contract(const Graph& g, const std::vector<int32_t>& match, std::vector<int
             if (x < 0) continue;
             vwsum += g.vw[x];
             for (int64_t e = g.rp[x]; e < g.rp[x + 1]; ++e) {
-                int32_t cu = cmap[g.ci[e]];
-                if (cu != c) row.push_back({cu, g.ew[e]});
+                const int32_t cu = cmap[g.ci[e]];
+                if (cu == c) continue;
+                if (stamp[cu] != c) {
+                    stamp[cu] = c;
+                    slot[cu] = (int64_t)cg.ci.size();
+                    cg.ci.push_back(cu);
+                    cg.ew.push_back(g.ew[e]);
+                } else {
+                    cg.ew[slot[cu]] += g.ew[e];
+                }
             }
         }
         cg.vw[c] = (int32_t)vwsum;
-        std::sort(row.begin(), row.end(), [](const std::pair<int32_t,int32_t>& a, const std::pair<int32_t,int32_t>& b){ return a.first < b.first; });
-        size_t i = 0;
-        while (i < row.size()) {
-            int64_t s = 0;
-            size_t j = i;
-            while (j < row.size() && row[j].first == row[i].first) { s += row[j].second; ++j; }
-            cg.ci.push_back(row[i].first);
-            cg.ew.push_back((int32_t)s);
-            i = j;
-        }
         cg.rp[c + 1] = (int64_t)cg.ci.size();
     }
 }
@@ -387,7 +386,7 @@ std::vector<int32_t> initial_partition(const Graph& g, const Params& P, int* bes
 //    such part); loss = conn(own) - conn(dest).  Candidates are ordered by
 //    (source part, loss bucket, id); a source keeps the prefix whose weight
 //    before the vertex is below its excess.  Weak mode then orders the kept
-//    moves by (dest, loss bucket, id) and keeps those that fit the
+//    moves by (dest, loss bucket, source, id) and keeps those that fit the
 //    destination's remaining capacity by an exclusive prefix sum; strong mode
 //    (after strong_after consecutive rebalance iterations) ignores the
 //    proposed destination and lays the kept moves, in source order, over the
@@ -397,8 +396,9 @@ std::vector<int32_t> initial_partition(const Graph& g, const Params& P, int* bes
 // state (balanced before unbalanced, then lower cut; unbalanced ones by lower
 // max part weight) is kept, as the reference keeps its best partition
 // (src/gpu_part.cu:627-631); the loop stops after refine_patience iterations
-// without a significant improvement (cut below 0.999 x best) or when label
-// propagation finds no move two iterations in a row.
+// without a significant improvement (cut below 0.999 x best), when label
+// propagation finds no move two iterations in a row, or when a strong
+// rebalance moves nothing (a weak one that moves nothing escalates to strong).
 struct Conn {
     std::vector<int64_t> c;
     std::vector<int32_t> touched;
@@ -498,6 +498,7 @@ void refine_level(const Graph& g, std::vector<int32_t>& part, const Params& P, i
                 std::sort(bd.begin(), bd.end(), [](const Cand& a, const Cand& b) {
                     if (a.d != b.d) return a.d < b.d;
                     if (a.bucket != b.bucket) return a.bucket < b.bucket;
+                    if (a.src != b.src) return a.src < b.src;
                     return a.v < b.v; });
                 size_t i = 0;
                 while (i < bd.size()) {
@@ -552,7 +553,13 @@ void refine_level(const Graph& g, std::vector<int32_t>& part, const Params& P, i
         stall = signif ? 0 : stall + 1;
         const bool lp_idle = (mode == 0 && nmoves == 0 && prev_moves == 0);
         prev_moves = nmoves;
-        if (stall >= P.o.refine_patience || lp_idle) { ++it; break; }
+        // a rebalance step that moved nothing is a fixed point of its mode:
+        // weak escalates to strong at once, strong ends the level
+        bool rb_stuck = false;
+        if (mode != 0 && nmoves == 0) {
+            if (mode == 1) rb_streak = P.o.strong_after; else rb_stuck = true;
+        }
+        if (stall >= P.o.refine_patience || lp_idle || rb_stuck) { ++it; break; }
     }
     part = best_part;
     if (iters_out) *iters_out += it;

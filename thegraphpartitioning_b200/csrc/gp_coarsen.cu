@@ -82,8 +82,12 @@ __device__ __forceinline__ void scan_best(const DGraph& g, int64_t v, int64_t be
     }
 }
 
+// Light rows: one warp per entry of the worklist `wl` (nullptr: every vertex,
+// wl_n = n); rows longer than kHeavyDeg are skipped there and handled by the
+// first nheavy CTAs, one row each.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_match_scan(DGraph g, const int32_t* __restrict__ heavy, int64_t nheavy,
+                                                    const int32_t* __restrict__ wl, int64_t wl_n,
                                                     const int32_t* __restrict__ match, int32_t* __restrict__ out,
                                                     uint64_t salt, int64_t maxvw,
                                                     uint64_t* __restrict__ list_keys, int64_t* __restrict__ list_cnt,
@@ -110,7 +114,8 @@ __global__ void __launch_bounds__(256) k_match_scan(DGraph g, const int32_t* __r
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)(gridDim.x - nheavy) * blockDim.x) >> 5;
-    for (int64_t v = wid; v < g.n; v += nw) {
+    for (int64_t i = wid; i < wl_n; i += nw) {
+        const int64_t v = wl ? wl[i] : i;
         const int64_t beg = g.rp[v], end = g.rp[v + 1];
         if (end - beg > kHeavyDeg) continue;
         if (match[v] != -1) { if (MODE == 0 && lane == 0) out[v] = -1; continue; }
@@ -122,15 +127,22 @@ __global__ void __launch_bounds__(256) k_match_scan(DGraph g, const int32_t* __r
     }
 }
 
-__global__ void k_handshake(int64_t n, const int32_t* __restrict__ prop, int32_t* __restrict__ match,
-                            int64_t* __restrict__ pairs) {
+// Mutual proposals become pairs; vertices left unmatched are appended to the
+// next round's worklist (any order: each vertex's proposal is its own).
+__global__ void k_handshake(const int32_t* __restrict__ wl, int64_t wl_n, const int32_t* __restrict__ prop,
+                            int32_t* __restrict__ match, int64_t* __restrict__ pairs,
+                            int32_t* __restrict__ next_wl, int64_t* __restrict__ next_n) {
     int64_t local = 0;
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < wl_n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = wl ? wl[i] : i;
         if (match[v] != -1) continue;
         const int32_t u = prop[v];
         if (u >= 0 && prop[u] == (int32_t)v) {
             match[v] = u;
             if (v < u) ++local;
+        } else {
+            unsigned long long slot = atomicAdd((unsigned long long*)next_n, 1ull);
+            next_wl[slot] = (int32_t)v;
         }
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
@@ -170,22 +182,31 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     const uint64_t salt = level_salt(P.seed, level);
     auto mk = c.tmp->save();
     int32_t* prop = c.tmp_alloc<int32_t>(g.n);
-    int64_t* d_pairs = c.tmp_alloc<int64_t>(2);
+    int32_t* wl[2] = {c.tmp_alloc<int32_t>(g.n), c.tmp_alloc<int32_t>(g.n)};
+    int64_t* d_pairs = c.tmp_alloc<int64_t>(4);
     GP_CUDA(cudaMemsetAsync(match, 0xff, sizeof(int32_t) * g.n, c.s));
     const int light_blocks = grid_for(g.n * 32, 256, c.sm_count * 8);
     const int grid = (int)L.nheavy + light_blocks;
     int64_t pairs = 0;
     int rounds = 0;
-    for (int r = 0; r < P.o.match_rounds; ++r) {
-        memset_async(c, d_pairs, 0, sizeof(int64_t));
-        k_match_scan<0><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, match, prop, salt, P.maxvw, nullptr, nullptr, 0);
+    const int32_t* cur = nullptr;   // round 0: every vertex
+    int64_t cur_n = g.n;
+    for (int r = 0; r < P.o.match_rounds && cur_n > 0; ++r) {
+        int32_t* next = wl[r & 1];
+        memset_async(c, d_pairs, 0, 2 * sizeof(int64_t));
+        k_match_scan<0><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, cur, cur_n, match, prop, salt, P.maxvw,
+                                               nullptr, nullptr, 0);
         GP_LAUNCHED(c);
-        k_handshake<<<grid_for(g.n, 256), 256, 0, c.s>>>(g.n, prop, match, d_pairs);
+        k_handshake<<<grid_for(cur_n, 256), 256, 0, c.s>>>(cur, cur_n, prop, match, d_pairs, next, d_pairs + 1);
         GP_LAUNCHED(c);
-        c.bytes += L.scan_bytes() + 4 * g.m /*match[u]*/ + 12 * g.n;
-        int64_t newp = read_i64(c, d_pairs);
+        c.bytes += (L.scan_bytes() + 4 * g.m) * cur_n / std::max<int64_t>(g.n, 1) + 16 * cur_n;
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_pairs, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        const int64_t newp = c.h_pinned[0];
         rounds = r + 1;
         pairs += newp;
+        cur = next;
+        cur_n = c.h_pinned[1];
         if (newp == 0) break;
     }
     if (P.o.two_hop > 0 && 4 * (g.n - pairs) > 3 * g.n) {
@@ -195,7 +216,8 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         int32_t* vals = c.tmp_alloc<int32_t>(g.n);
         int32_t* vals2 = c.tmp_alloc<int32_t>(g.n);
         memset_async(c, d_pairs, 0, 2 * sizeof(int64_t));
-        k_match_scan<1><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, match, nullptr, salt, P.maxvw, keys, d_pairs + 1, nb);
+        k_match_scan<1><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, nullptr, g.n, match, nullptr, salt, P.maxvw,
+                                               keys, d_pairs + 1, nb);
         GP_LAUNCHED(c);
         c.bytes += L.scan_bytes() + 4 * g.n;
         int64_t cnt = read_i64(c, d_pairs + 1);
@@ -243,55 +265,208 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
     }
 }
 
-// warp per coarse vertex: write (c << nb | cmap[u], w) for every entry of its members' rows
-__global__ void __launch_bounds__(256) k_fill(DGraph g, int64_t nc, const int32_t* __restrict__ mem,
-                                              const int32_t* __restrict__ cmap, const int64_t* __restrict__ off,
-                                              int nb, uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+// ---- row dedup in first-occurrence order
+// Coarse row c walks N(a) then N(b) (a = representative, b = partner) in CSR
+// order; position j in that walk.  Every coarse neighbour is kept once, at
+// the rank of its first position, with the weights of all its positions
+// summed; c itself is dropped.
+constexpr int SMALL_ROW = 128;          // rows up to this length: one warp, 256-slot table
+constexpr int SMALL_SLOTS = 256;
+constexpr int BIG_T = 256;              // threads of the CTA per longer row
+constexpr int SMEM_SLOTS = 4096;        // longer rows with <= 2048 entries keep their table on chip
+constexpr int32_t EMPTY_KEY = -1;
+
+__device__ __forceinline__ uint32_t slot_hash(int32_t key, int lg) {
+    return ((uint32_t)key * 0x9E3779B1u) >> (32 - lg);
+}
+
+__device__ __forceinline__ void row_entry(const DGraph& g, int32_t a, int32_t b, int64_t da, int64_t j,
+                                          const int32_t* __restrict__ cmap, int32_t& cu, int32_t& w) {
+    const int64_t e = j < da ? g.rp[a] + j : g.rp[b] + (j - da);
+    cu = cmap[g.ci[e]];
+    w = g.ew ? g.ew[e] : 1;
+}
+
+// one warp per coarse row with at most SMALL_ROW entries; table in shared memory
+__global__ void __launch_bounds__(256) k_contract_small(DGraph g, int64_t nc, const int32_t* __restrict__ mem,
+                                                        const int32_t* __restrict__ cmap, const int64_t* __restrict__ off,
+                                                        const int64_t* __restrict__ cdeg, int32_t* __restrict__ tci,
+                                                        int32_t* __restrict__ tew, int32_t* __restrict__ cnt) {
+    __shared__ int32_t s_key[8][SMALL_SLOTS];
+    __shared__ int32_t s_idx[8][SMALL_SLOTS];
+    __shared__ int32_t s_okey[8][SMALL_ROW];
+    __shared__ int32_t s_w[8][SMALL_ROW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t* key = s_key[w];
+    int32_t* tidx = s_idx[w];
+    int32_t* okey = s_okey[w];
+    int32_t* wacc = s_w[w];
+    for (int i = lane; i < SMALL_SLOTS; i += 32) key[i] = EMPTY_KEY;
+    for (int i = lane; i < SMALL_ROW; i += 32) wacc[i] = 0;
+    __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = wid; c < nc; c += nw) {
+        const int64_t deg = cdeg[c];
+        if (deg > SMALL_ROW) continue;
+        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
+        const int64_t da = g.rp[a + 1] - g.rp[a];
+        int32_t count = 0;
+        for (int64_t base = 0; base < deg; base += 32) {
+            const int64_t j = base + lane;
+            int32_t cu = -1, wt = 0;
+            if (j < deg) row_entry(g, a, b, da, j, cmap, cu, wt);
+            const bool act = (j < deg) && cu != (int32_t)c;
+            const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
+            const int leader = __ffs(peers) - 1;
+            bool isnew = false;
+            int32_t h = -1;
+            if (act && lane == leader) {
+                h = (int32_t)slot_hash(cu, 8);
+                for (int probe = 0; probe < SMALL_SLOTS; ++probe) {
+                    const int32_t old = atomicCAS(&key[h], EMPTY_KEY, cu);
+                    if (old == EMPTY_KEY) { isnew = true; break; }
+                    if (old == cu) break;
+                    h = (h + 1) & (SMALL_SLOTS - 1);
+                }
+            }
+            const uint32_t newmask = __ballot_sync(0xffffffffu, isnew);
+            int32_t idx = -1;
+            if (isnew) {
+                idx = count + __popc(newmask & lt);
+                tidx[h] = idx;
+                okey[idx] = cu;
+            }
+            __syncwarp();
+            if (act && lane == leader && !isnew) idx = tidx[h];
+            idx = __shfl_sync(0xffffffffu, idx, leader);
+            if (act) atomicAdd(&wacc[idx], wt);
+            count += __popc(newmask);
+            __syncwarp();
+        }
+        const int64_t o = off[c];
+        for (int i = lane; i < count; i += 32) {
+            tci[o + i] = okey[i];
+            tew[o + i] = wacc[i];
+            wacc[i] = 0;
+        }
+        for (int i = lane; i < SMALL_SLOTS; i += 32) key[i] = EMPTY_KEY;
+        if (lane == 0) cnt[c] = count;
+        __syncwarp();
+    }
+}
+
+__global__ void k_big_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ list,
+                           int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = cdeg[c];
+        if (d <= SMALL_ROW) continue;
+        unsigned long long slot = atomicAdd((unsigned long long*)count, 1ull);
+        list[slot] = (int32_t)c;
+        int64_t S = 1;
+        while (S < 2 * d) S <<= 1;
+        tsize[slot] = S > SMEM_SLOTS ? S : 0;
+    }
+}
+
+__device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32_t& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) { int32_t y = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += y; }
+    if (lane == 31) sh[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int32_t s2 = lane < nw ? sh[lane] : 0, i2 = s2;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { int32_t y = __shfl_up_sync(0xffffffffu, i2, o); if (lane >= o) i2 += y; }
+        if (lane < nw) sh[lane] = i2 - s2;
+        if (lane == nw - 1) sh[32] = i2;
+    }
+    __syncthreads();
+    const int32_t r = inc - x + sh[w];
+    total = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// one CTA per longer row: hash table on chip (<= SMEM_SLOTS slots) or in the
+// global region toff; phase 1 inserts (first position by atomicMin, weights by
+// atomicAdd), phase 2 ranks first positions with a block scan in row order.
+__global__ void __launch_bounds__(BIG_T) k_contract_big(DGraph g, const int32_t* __restrict__ list, int64_t nbig,
+                                                        const int32_t* __restrict__ mem, const int32_t* __restrict__ cmap,
+                                                        const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
+                                                        const int64_t* __restrict__ toff, int32_t* __restrict__ gtab,
+                                                        int32_t* __restrict__ tci, int32_t* __restrict__ tew,
+                                                        int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+    extern __shared__ int32_t stab[];
+    __shared__ int32_t sh[33];
+    for (int64_t li = blockIdx.x; li < nbig; li += gridDim.x) {
+        const int64_t c = list[li];
+        const int64_t deg = cdeg[c];
+        int64_t S = 1;
+        int lg = 0;
+        while (S < 2 * deg) { S <<= 1; ++lg; }
+        int32_t* keys = S <= SMEM_SLOTS ? stab : gtab + 3 * toff[li];
+        int32_t* minpos = keys + S;
+        int32_t* wsum = minpos + S;
+        for (int64_t i = threadIdx.x; i < S; i += BIG_T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
+        __syncthreads();
+        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
+        const int64_t da = g.rp[a + 1] - g.rp[a];
+        for (int64_t j = threadIdx.x; j < deg; j += BIG_T) {
+            int32_t cu, wt;
+            row_entry(g, a, b, da, j, cmap, cu, wt);
+            if (cu == (int32_t)c) continue;
+            uint32_t h = slot_hash(cu, lg);
+            bool placed = false;
+            for (int64_t probe = 0; probe < S; ++probe) {
+                const int32_t old = atomicCAS(&keys[h], EMPTY_KEY, cu);
+                if (old == EMPTY_KEY || old == cu) { placed = true; break; }
+                h = (h + 1) & (uint32_t)(S - 1);
+            }
+            if (!placed) { atomicExch(err, 1); continue; }
+            atomicMin(&minpos[h], (int32_t)j);
+            atomicAdd(&wsum[h], wt);
+        }
+        __syncthreads();
+        int32_t carry = 0;
+        const int64_t o = off[c];
+        for (int64_t base = 0; base < deg; base += BIG_T) {
+            const int64_t j = base + threadIdx.x;
+            int32_t first = 0, cu = -1;
+            uint32_t h = 0;
+            if (j < deg) {
+                int32_t wt;
+                row_entry(g, a, b, da, j, cmap, cu, wt);
+                if (cu != (int32_t)c) {
+                    h = slot_hash(cu, lg);
+                    for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
+                    first = (keys[h] == cu && minpos[h] == (int32_t)j) ? 1 : 0;
+                }
+            }
+            int32_t tot;
+            const int32_t r = block_scan_excl(first, sh, tot);
+            if (first) { tci[o + carry + r] = cu; tew[o + carry + r] = wsum[h]; }
+            carry += tot;
+        }
+        if (threadIdx.x == 0) cnt[c] = carry;
+        __syncthreads();
+    }
+}
+
+// warp per coarse row: temporary (row bound offsets) -> final CSR
+__global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, const int64_t* __restrict__ off,
+                                                       const int64_t* __restrict__ crp, const int32_t* __restrict__ tci,
+                                                       const int32_t* __restrict__ tew, int32_t* __restrict__ ci,
+                                                       int32_t* __restrict__ ew) {
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t cc = wid; cc < nc; cc += nw) {
-        int64_t pos = off[cc];
-        const uint64_t hi = (uint64_t)cc << nb;
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-            const int32_t x = mem[2 * cc + t];
-            if (x < 0) continue;
-            const int64_t beg = g.rp[x], end = g.rp[x + 1];
-            for (int64_t e = beg + lane; e < end; e += 32) {
-                keys[pos + (e - beg)] = hi | (uint32_t)cmap[g.ci[e]];
-                vals[pos + (e - beg)] = g.ew ? g.ew[e] : 1;
-            }
-            pos += end - beg;
-        }
-    }
-}
-
-// unique flags over sorted keys: first of a run and not a self-loop
-__global__ void k_uniq_flags(const uint64_t* __restrict__ keys, int64_t T, int nb, int32_t* __restrict__ flag,
-                             int32_t* __restrict__ rowcnt) {
-    const uint64_t lowmask = (1ull << nb) - 1;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = keys[i];
-        const bool head = (i == 0) || (keys[i - 1] != k);
-        const bool self = (k >> nb) == (k & lowmask);
-        const int f = (head && !self) ? 1 : 0;
-        flag[i] = f;
-        if (f) atomicAdd(&rowcnt[k >> nb], 1);
-    }
-}
-
-__global__ void k_uniq_write(const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals, int64_t T, int nb,
-                             const int32_t* __restrict__ flag, const int64_t* __restrict__ pos,
-                             int32_t* __restrict__ ci, int32_t* __restrict__ ew) {
-    const uint64_t lowmask = (1ull << nb) - 1;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += (int64_t)gridDim.x * blockDim.x) {
-        if (!flag[i]) continue;
-        const uint64_t k = keys[i];
-        int64_t s = vals[i];
-        for (int64_t j = i + 1; j < T && keys[j] == k; ++j) s += vals[j];
-        ci[pos[i]] = (int32_t)(k & lowmask);
-        ew[pos[i]] = (int32_t)s;
+    for (int64_t c = wid; c < nc; c += nw) {
+        const int64_t src = off[c], dst = crp[c], len = crp[c + 1] - crp[c];
+        for (int64_t i = lane; i < len; i += 32) { ci[dst + i] = tci[src + i]; ew[dst + i] = tew[src + i]; }
     }
 }
 
@@ -311,32 +486,48 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int64_t* cdeg = c.tmp_alloc<int64_t>(nc);
     k_cmap<<<grid_for(g.n, 256), 256, 0, c.s>>>(g, match, cid, fine.cmap, mem, cvw, cdeg);
     GP_LAUNCHED(c);
-    int64_t* off = c.tmp_alloc<int64_t>(nc);
-    scan_excl_i64(c, cdeg, off, nc, d_tot + 1);
+    int64_t* off = c.tmp_alloc<int64_t>(nc + 1);
+    scan_excl_i64(c, cdeg, off, nc, off + nc);
     const int64_t T = g.m;
-    const int nb = bits_for(nc);
-    uint64_t* keys = c.tmp_alloc<uint64_t>(T);
-    int32_t* vals = c.tmp_alloc<int32_t>(T);
-    uint64_t* keys2 = c.tmp_alloc<uint64_t>(T);
-    int32_t* vals2 = c.tmp_alloc<int32_t>(T);
-    k_fill<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(g, nc, mem, fine.cmap, off, nb, keys, vals);
-    GP_LAUNCHED(c);
-    radix_sort_pairs(c, keys, vals, keys2, vals2, T, 2 * nb);
-    int32_t* uflag = c.tmp_alloc<int32_t>(T);
+    int32_t* tci = c.tmp_alloc<int32_t>(T);
+    int32_t* tew = c.tmp_alloc<int32_t>(T);
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
-    int64_t* upos = c.tmp_alloc<int64_t>(T);
-    memset_async(c, rowcnt, 0, sizeof(int32_t) * nc);
-    k_uniq_flags<<<grid_for(T, 256), 256, 0, c.s>>>(keys, T, nb, uflag, rowcnt);
+    int32_t* blist = c.tmp_alloc<int32_t>(nc);
+    int64_t* tsize = c.tmp_alloc<int64_t>(nc + 1);
+    int32_t* err = c.tmp_alloc<int32_t>(1);
+    memset_async(c, d_tot + 1, 0, sizeof(int64_t));
+    memset_async(c, err, 0, sizeof(int32_t));
+    k_contract_small<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(g, nc, mem, fine.cmap, off, cdeg, tci,
+                                                                             tew, rowcnt);
     GP_LAUNCHED(c);
-    scan_excl_i32_to_i64(c, uflag, upos, T, d_tot + 2);
-    const int64_t mc = read_i64(c, d_tot + 2);
+    k_big_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, blist, tsize, d_tot + 1);
+    GP_LAUNCHED(c);
+    const int64_t nbig = read_i64(c, d_tot + 1);
+    if (nbig > 0) {
+        int64_t* toff = c.tmp_alloc<int64_t>(nbig + 1);
+        scan_excl_i64(c, tsize, toff, nbig, toff + nbig);
+        const int64_t tslots = read_i64(c, toff + nbig);
+        int32_t* gtab = c.tmp_alloc<int32_t>(3 * std::max<int64_t>(tslots, 1));
+        const size_t smem = 3 * sizeof(int32_t) * SMEM_SLOTS;
+        GP_CUDA(cudaFuncSetAttribute(k_contract_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_contract_big<<<(unsigned)std::min<int64_t>(nbig, (int64_t)c.sm_count * 4), BIG_T, smem, c.s>>>(
+            g, blist, nbig, mem, fine.cmap, off, cdeg, toff, gtab, tci, tew, rowcnt, err);
+        GP_LAUNCHED(c);
+    }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);
     scan_excl_i32_to_i64(c, rowcnt, crp, nc, crp + nc);
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, crp + nc, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned + 1, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+    c.sync();
+    const int64_t mc = c.h_pinned[0];
+    if ((int32_t)c.h_pinned[1] != 0) throw GpError(GP_EINTERNAL, "contraction hash table overflow");
     int32_t* cci = c.keep_alloc<int32_t>(mc);
     int32_t* cew = c.keep_alloc<int32_t>(mc);
-    k_uniq_write<<<grid_for(T, 256), 256, 0, c.s>>>(keys, vals, T, nb, uflag, upos, cci, cew);
+    k_contract_copy<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(nc, off, crp, tci, tew, cci, cew);
     GP_LAUNCHED(c);
-    c.bytes += 2 * (8 * (g.n + 1) + 8 * g.m) + 8 * (nc + 1) + 8 * mc + 4 * nc + 12 * T;
+    // rows read twice (count and rank for long rows), cmap gathered per entry,
+    // unique entries written to the temporary and copied once
+    c.bytes += 2 * (8 * (g.n + 1) + 8 * g.m) + 4 * g.m + 8 * (nc + 1) + 4 * nc + 24 * mc + 24 * nc;
     coarse.g.n = nc;
     coarse.g.m = mc;
     coarse.g.rp = crp;

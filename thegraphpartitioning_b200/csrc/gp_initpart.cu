@@ -49,11 +49,14 @@ __device__ void ip_bfs(const DGraph& g, const int32_t* lab, int32_t* dist, const
     const int64_t n = g.n;
     if (threadIdx.x == 0) { flags[0] = 0; flags[1] = 0; flags[2] = 0; }
     __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int32_t r = 0;; ++r) {
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+        // one warp per frontier vertex: rows of the coarsest graph can be long
+        for (int64_t v = wid; v < n; v += nw) {
             const int32_t L = lab[v];
             if (S.cnt_d[L] <= 1 || dist[v] != r) continue;
-            for (int64_t e = g.rp[v]; e < g.rp[v + 1]; ++e) {
+            for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32) {
                 const int32_t u = g.ci[e];
                 if (lab[u] == L && dist[u] == IP_INF) { dist[u] = r + 1; flags[r % 3] = 1; }
             }
@@ -190,11 +193,14 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
     for (int q = threadIdx.x; q < k; q += blockDim.x) S.WL[q] = 0;
     __syncthreads();
     int64_t cross = 0;
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const int32_t p = lab[v];
-        atomicAdd((unsigned long long*)&S.WL[p], (unsigned long long)(g.vw ? g.vw[v] : 1));
-        for (int64_t e = g.rp[v]; e < g.rp[v + 1]; ++e)
-            if (lab[g.ci[e]] != p) cross += g.ew ? g.ew[e] : 1;
+    {
+        const int lane = threadIdx.x & 31;
+        for (int64_t v = threadIdx.x >> 5; v < n; v += blockDim.x >> 5) {
+            const int32_t p = lab[v];
+            if (lane == 0) atomicAdd((unsigned long long*)&S.WL[p], (unsigned long long)(g.vw ? g.vw[v] : 1));
+            for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32)
+                if (lab[g.ci[e]] != p) cross += g.ew ? g.ew[e] : 1;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) cross += __shfl_xor_sync(0xffffffffu, cross, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cross;

@@ -57,13 +57,14 @@ __device__ __forceinline__ bool lp_candidate(int64_t g, int64_t own, int32_t den
 
 // ------------------------------------------------------------------ k_conn
 // status: [S_CROSS] += directed cross weight, [S_MAXPW], [S_MODE], [S_LIGHT] written by CTA 0,
-// [S_NCAND] rebalance candidates appended to ckeys/cvals, [S_NLIST] LP candidates appended to clist.
+// [S_NLIST] LP candidates appended to clist (any order: each is evaluated on its own).
+// Rebalance candidates are the vertices with dest >= 0; they are compacted in
+// vertex order afterwards (k_rb_flags + scan + k_rb_compact).
 __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, int32_t den, int force_eval,
                                              const int32_t* __restrict__ part, const uint8_t* __restrict__ lock,
                                              const int64_t* __restrict__ pw, const int32_t* __restrict__ heavy,
                                              int64_t nheavy, int32_t* __restrict__ dest, int32_t* __restrict__ gain,
-                                             int64_t* __restrict__ status, uint64_t* __restrict__ ckeys,
-                                             int32_t* __restrict__ cvals, int32_t* __restrict__ clist) {
+                                             int64_t* __restrict__ status, int32_t* __restrict__ clist) {
     extern __shared__ int32_t csm[];
     const int kpad = (k + 15) & ~15;
     uint8_t* over = (uint8_t*)csm;
@@ -152,11 +153,7 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
             } else if (mode == MODE_RB && active) {
                 const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
                 d = bq >= 0 ? bq : light;
-                const int32_t loss = (int32_t)(own - cd);
-                gn = -loss;
-                unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NCAND], 1ull);
-                ckeys[slot] = ((uint64_t)p << 41) | ((uint64_t)loss_bucket(loss) << 31) | (uint64_t)v;
-                cvals[slot] = (int32_t)v;
+                gn = -(int32_t)(own - cd);
             }
             dest[v] = d; gain[v] = gn;
         }
@@ -210,11 +207,7 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
                 } else {
                     const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
                     d = bq >= 0 ? bq : light;
-                    const int32_t loss = (int32_t)(own - cd);
-                    gn = -loss;
-                    unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NCAND], 1ull);
-                    ckeys[slot] = ((uint64_t)p << 41) | ((uint64_t)loss_bucket(loss) << 31) | (uint64_t)v;
-                    cvals[slot] = (int32_t)v;
+                    gn = -(int32_t)(own - cd);
                 }
                 dest[v] = d; gain[v] = gn;
             }
@@ -321,11 +314,30 @@ __global__ void k_gather_vw(int64_t cnt, const int32_t* __restrict__ vidx, const
         out[i] = vw ? vw[vidx[i]] : 1;
 }
 
+constexpr int RB_SHIFT = 10;   // key = segment << 10 | loss bucket
+
+__global__ void k_rb_flags(int64_t n, const int32_t* __restrict__ dest, int32_t* __restrict__ flag) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        flag[v] = dest[v] >= 0 ? 1 : 0;
+}
+
+// candidates in vertex order with key (source << 10 | bucket(loss))
+__global__ void k_rb_compact(int64_t n, const int32_t* __restrict__ flag, const int64_t* __restrict__ pos,
+                             const int32_t* __restrict__ part, const int32_t* __restrict__ gain,
+                             uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        if (!flag[v]) continue;
+        const int64_t i = pos[v];
+        keys[i] = ((uint64_t)(uint32_t)part[v] << RB_SHIFT) | loss_bucket(-gain[v]);
+        vals[i] = (int32_t)v;
+    }
+}
+
 __device__ __forceinline__ int64_t seg_start(const uint64_t* keys, int64_t i, uint64_t seg) {
     int64_t lo = 0, hi = i;
     while (lo < hi) {
         int64_t mid = (lo + hi) >> 1;
-        if ((keys[mid] >> 41) < seg) lo = mid + 1; else hi = mid;
+        if ((keys[mid] >> RB_SHIFT) < seg) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
@@ -334,23 +346,22 @@ __device__ __forceinline__ int64_t seg_start(const uint64_t* keys, int64_t i, ui
 __global__ void k_rb_source(int64_t cnt, const uint64_t* __restrict__ keys, const int64_t* __restrict__ pre,
                             const int64_t* __restrict__ pw, int64_t Lmax, int32_t* __restrict__ flag) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t src = keys[i] >> 41;
+        const uint64_t src = keys[i] >> RB_SHIFT;
         const int64_t s = seg_start(keys, i, src);
         flag[i] = (pre[i] - pre[s]) < (pw[src] - Lmax) ? 1 : 0;
     }
 }
 
-// weak: re-key accepted moves by destination
+// weak: accepted moves, in list order, re-keyed by (dest << 10 | bucket)
 __global__ void k_rb_rekey(int64_t cnt, const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals,
-                           const int32_t* __restrict__ flag, const int32_t* __restrict__ dest,
-                           uint64_t* __restrict__ keys2, int32_t* __restrict__ vals2, int64_t* __restrict__ cnt2) {
+                           const int32_t* __restrict__ flag, const int64_t* __restrict__ pos,
+                           const int32_t* __restrict__ dest, uint64_t* __restrict__ keys2, int32_t* __restrict__ vals2) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
         const int32_t v = vals[i];
-        const uint64_t low = keys[i] & ((1ull << 41) - 1);  // bucket | id
-        unsigned long long slot = atomicAdd((unsigned long long*)cnt2, 1ull);
-        keys2[slot] = ((uint64_t)(uint32_t)dest[v] << 41) | low;
-        vals2[slot] = v;
+        const int64_t j = pos[i];
+        keys2[j] = ((uint64_t)(uint32_t)dest[v] << RB_SHIFT) | (keys[i] & ((1ull << RB_SHIFT) - 1));
+        vals2[j] = v;
     }
 }
 
@@ -360,7 +371,7 @@ __global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, 
                                 const int64_t* __restrict__ pw_snap, int64_t Lmax, int32_t* __restrict__ part,
                                 uint8_t* __restrict__ lock, int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t d = keys[i] >> 41;
+        const uint64_t d = keys[i] >> RB_SHIFT;
         const int64_t s = seg_start(keys, i, d);
         const int32_t v = vals[i];
         const int64_t wv = vw ? vw[v] : 1;
@@ -516,7 +527,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const int light_blocks = grid_for(n * 32, RT, c.sm_count * 8);
     const int grid = (int)L.nheavy + light_blocks;
     int64_t best_cut = 0, best_mp = 0;
-    int stall = 0, rb_streak = 0, steps = 0, last_mode = MODE_LP;
+    int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
     int64_t prev_moves = -1;
     const int nb_k = bits_for(k);
     for (int it = 0;; ++it) {
@@ -524,7 +535,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         GP_CUDA(cudaMemsetAsync(B.status, 0, sizeof(int64_t) * S_NRESET, c.s));
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_a, c.s));
         k_conn<<<grid, RT, conn_smem, c.s>>>(g, k, Lmax, P.o.lp_filter_den, final_eval ? 1 : 0, B.part, B.lock, B.pw,
-                                             L.heavy, L.nheavy, B.dest, B.gain, B.status, B.ckeys, B.cvals, B.clist);
+                                             L.heavy, L.nheavy, B.dest, B.gain, B.status, B.clist);
         GP_LAUNCHED(c);
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_b, c.s));
         // rowptr, colidx, weights, gathered part[u]; part[v], lock[v] read; dest, gain written
@@ -542,7 +553,6 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         const int64_t cur_cut = c.h_pinned[S_CROSS] / 2;
         const int64_t cur_mp = c.h_pinned[S_MAXPW];
         const int dev_mode = (int)c.h_pinned[S_MODE];
-        const int64_t ncand = c.h_pinned[S_NCAND];
         const int64_t nlist = c.h_pinned[S_NLIST];
         const int64_t cdeg = c.h_pinned[S_CDEG];
         if (it == 0) {
@@ -562,15 +572,20 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                 GP_CUDA(cudaMemcpyAsync(B.best_pw, B.pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
             }
             stall = signif ? 0 : stall + 1;
-            const bool lp_idle = (last_mode == MODE_LP && nmoves == 0 && prev_moves == 0);
+            const bool lp_idle = (last_mode == 0 && nmoves == 0 && prev_moves == 0);
             prev_moves = nmoves;
-            if (stall >= P.o.refine_patience || lp_idle) break;
+            // a rebalance step that moved nothing: weak escalates to strong, strong ends the level
+            bool rb_stuck = false;
+            if (last_mode != 0 && nmoves == 0) {
+                if (last_mode == 1) rb_streak = P.o.strong_after; else rb_stuck = true;
+            }
+            if (stall >= P.o.refine_patience || lp_idle || rb_stuck) break;
         }
         if (final_eval) break;
         int mode;
         if (dev_mode == MODE_RB) { mode = (rb_streak >= P.o.strong_after) ? 2 : 1; ++rb_streak; }
         else { mode = 0; rb_streak = 0; }
-        last_mode = (mode == 0) ? MODE_LP : MODE_RB;
+        last_mode = mode;
         int64_t* moves_d = B.status + S_STEP_MOVES;  // moves of this step, read at the next sync
         memset_async(c, moves_d, 0, sizeof(int64_t));
         if (mode == 0) {
@@ -585,28 +600,38 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             std::swap(B.lock, B.lock_next);
         } else {
             memset_async(c, B.lock, 0, n);
+            auto mk = c.tmp->save();
+            // candidates (dest >= 0) in vertex order, keyed (source, bucket); stable sort -> (source, bucket, id)
+            int32_t* flag = c.tmp_alloc<int32_t>(n);
+            int64_t* vpos = c.tmp_alloc<int64_t>(n + 1);
+            k_rb_flags<<<grid_for(n, 256), 256, 0, c.s>>>(n, B.dest, flag);
+            GP_LAUNCHED(c);
+            scan_excl_i32_to_i64(c, flag, vpos, n, vpos + n);
+            const int64_t ncand = read_i64(c, vpos + n);
+            c.bytes += 4 * n + 12 * n;
             if (ncand > 0) {
-                auto mk = c.tmp->save();
-                const int bits = 41 + nb_k;
+                k_rb_compact<<<grid_for(n, 256), 256, 0, c.s>>>(n, flag, vpos, B.part, B.gain, B.ckeys, B.cvals);
+                GP_LAUNCHED(c);
+                const int bits = RB_SHIFT + nb_k;
                 radix_sort_pairs(c, B.ckeys, B.cvals, B.ckeys2, B.cvals2, ncand, bits);
                 int32_t* wv = c.tmp_alloc<int32_t>(ncand);
-                int64_t* pre = c.tmp_alloc<int64_t>(ncand);
-                int32_t* flag = c.tmp_alloc<int32_t>(ncand);
+                int64_t* pre = c.tmp_alloc<int64_t>(ncand + 1);
+                int32_t* acc = c.tmp_alloc<int32_t>(ncand);
                 int64_t* pw_snap = c.tmp_alloc<int64_t>(k);
                 GP_CUDA(cudaMemcpyAsync(pw_snap, B.pw, sizeof(int64_t) * k, cudaMemcpyDeviceToDevice, c.s));
                 k_gather_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, g.vw, wv);
                 GP_LAUNCHED(c);
                 scan_excl_i32_to_i64(c, wv, pre, ncand, nullptr);
-                k_rb_source<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, pre, B.pw, Lmax, flag);
+                k_rb_source<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, pre, B.pw, Lmax, acc);
                 GP_LAUNCHED(c);
                 if (mode == 1) {
-                    int64_t* cnt2 = c.tmp_alloc<int64_t>(1);
-                    memset_async(c, cnt2, 0, sizeof(int64_t));
-                    k_rb_rekey<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, B.cvals, flag, B.dest,
-                                                                    B.ckeys2, B.cvals2, cnt2);
-                    GP_LAUNCHED(c);
-                    const int64_t n2 = read_i64(c, cnt2);
+                    int64_t* apos = c.tmp_alloc<int64_t>(ncand + 1);
+                    scan_excl_i32_to_i64(c, acc, apos, ncand, apos + ncand);
+                    const int64_t n2 = read_i64(c, apos + ncand);
                     if (n2 > 0) {
+                        k_rb_rekey<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, B.cvals, acc, apos, B.dest,
+                                                                        B.ckeys2, B.cvals2);
+                        GP_LAUNCHED(c);
                         radix_sort_pairs(c, B.ckeys2, B.cvals2, B.ckeys, B.cvals, n2, bits);
                         k_gather_vw<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.cvals2, g.vw, wv);
                         GP_LAUNCHED(c);
@@ -620,16 +645,16 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                     int32_t* wm = c.tmp_alloc<int32_t>(ncand);
                     k_cumfree<<<1, 32, 0, c.s>>>(k, B.pw, Lmax, cum);
                     GP_LAUNCHED(c);
-                    k_mask_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, flag, wv, wm);
+                    k_mask_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, acc, wv, wm);
                     GP_LAUNCHED(c);
                     scan_excl_i32_to_i64(c, wm, pre, ncand, nullptr);
-                    k_rb_strong_apply<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, flag, pre, g.vw, cum, k,
+                    k_rb_strong_apply<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, acc, pre, g.vw, cum, k,
                                                                            B.part, B.lock, B.pw, moves_d);
                     GP_LAUNCHED(c);
                 }
-                c.bytes += 60 * ncand;
-                c.tmp->restore(mk);
+                c.bytes += 80 * ncand;
             }
+            c.tmp->restore(mk);
         }
         ++steps;
         if (tr.on()) trace_iter(c, B, n, g.m, level, it, mode, cur_cut, cur_mp, tr);
