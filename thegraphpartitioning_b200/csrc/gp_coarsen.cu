@@ -270,10 +270,11 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // order; position j in that walk.  Every coarse neighbour is kept once, at
 // the rank of its first position, with the weights of all its positions
 // summed; c itself is dropped.
-constexpr int SMALL_ROW = 128;          // rows up to this length: one warp, 256-slot table
+constexpr int SMALL_ROW = 128;          // rows up to this length: one warp, 256-slot table on chip
 constexpr int SMALL_SLOTS = 256;
-constexpr int BIG_T = 256;              // threads of the CTA per longer row
-constexpr int SMEM_SLOTS = 4096;        // longer rows with <= 2048 entries keep their table on chip
+constexpr int MID_ROW = 8192;           // rows up to this length: one warp, private table in global memory
+constexpr int MID_SLOTS = 2 * MID_ROW;
+constexpr int BIG_T = 1024;             // longer rows: one CTA each, two-phase
 constexpr int32_t EMPTY_KEY = -1;
 
 __device__ __forceinline__ uint32_t slot_hash(int32_t key, int lg) {
@@ -357,19 +358,6 @@ __global__ void __launch_bounds__(256) k_contract_small(DGraph g, int64_t nc, co
     }
 }
 
-__global__ void k_big_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ list,
-                           int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t d = cdeg[c];
-        if (d <= SMALL_ROW) continue;
-        unsigned long long slot = atomicAdd((unsigned long long*)count, 1ull);
-        list[slot] = (int32_t)c;
-        int64_t S = 1;
-        while (S < 2 * d) S <<= 1;
-        tsize[slot] = S > SMEM_SLOTS ? S : 0;
-    }
-}
-
 __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32_t& total) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     int32_t inc = x;
@@ -391,16 +379,101 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
     return r;
 }
 
-// one CTA per longer row: hash table on chip (<= SMEM_SLOTS slots) or in the
-// global region toff; phase 1 inserts (first position by atomicMin, weights by
-// atomicAdd), phase 2 ranks first positions with a block scan in row order.
+// rows of SMALL_ROW < d <= MID_ROW go to list1, longer ones to list2 (with
+// the size of their global table); list order is irrelevant (rows are independent)
+__global__ void k_big_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ list1,
+                           int32_t* __restrict__ list2, int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = cdeg[c];
+        if (d <= SMALL_ROW) continue;
+        if (d <= MID_ROW) {
+            unsigned long long slot = atomicAdd((unsigned long long*)&count[0], 1ull);
+            list1[slot] = (int32_t)c;
+        } else {
+            unsigned long long slot = atomicAdd((unsigned long long*)&count[1], 1ull);
+            list2[slot] = (int32_t)c;
+            int64_t S = 1;
+            while (S < 2 * d) S <<= 1;
+            tsize[slot] = S;
+        }
+    }
+}
+
+// one warp per row of list1, chunks of 32 entries in row order; the table
+// (key, output rank) lives in the warp's private global region (L2 resident),
+// output entries and weights go straight to the temporary row.
+__global__ void __launch_bounds__(256) k_contract_mid(DGraph g, const int32_t* __restrict__ list, int64_t nlist,
+                                                      const int32_t* __restrict__ mem, const int32_t* __restrict__ cmap,
+                                                      const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
+                                                      int32_t* __restrict__ wtab, int32_t* __restrict__ tci,
+                                                      int32_t* __restrict__ tew, int32_t* __restrict__ cnt,
+                                                      int32_t* __restrict__ err) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int32_t* key = wtab + wid * (2 * (int64_t)MID_SLOTS);
+    int32_t* tidx = key + MID_SLOTS;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int64_t li = wid; li < nlist; li += nw) {
+        const int64_t c = list[li];
+        const int64_t deg = cdeg[c];
+        int S = 1, lg = 0;
+        while (S < 2 * deg) { S <<= 1; ++lg; }
+        for (int i = lane; i < S; i += 32) key[i] = EMPTY_KEY;
+        __syncwarp();
+        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
+        const int64_t da = g.rp[a + 1] - g.rp[a];
+        const int64_t o = off[c];
+        int32_t count = 0;
+        for (int64_t base = 0; base < deg; base += 32) {
+            const int64_t j = base + lane;
+            int32_t cu = -1, wt = 0;
+            if (j < deg) row_entry(g, a, b, da, j, cmap, cu, wt);
+            const bool act = (j < deg) && cu != (int32_t)c;
+            const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
+            const int leader = __ffs(peers) - 1;
+            bool isnew = false;
+            int32_t h = -1;
+            if (act && lane == leader) {
+                h = (int32_t)slot_hash(cu, lg);
+                bool placed = false;
+                for (int probe = 0; probe < S; ++probe) {
+                    const int32_t old = atomicCAS(&key[h], EMPTY_KEY, cu);
+                    if (old == EMPTY_KEY) { isnew = true; placed = true; break; }
+                    if (old == cu) { placed = true; break; }
+                    h = (h + 1) & (S - 1);
+                }
+                if (!placed) atomicExch(err, 1);
+            }
+            const uint32_t newmask = __ballot_sync(0xffffffffu, isnew);
+            int32_t idx = -1;
+            if (isnew) {
+                idx = count + __popc(newmask & lt);
+                tidx[h] = idx;
+                tci[o + idx] = cu;
+                tew[o + idx] = 0;
+            }
+            __syncwarp();
+            if (act && lane == leader && !isnew && h >= 0) idx = tidx[h];
+            idx = __shfl_sync(0xffffffffu, idx, leader);
+            if (act && idx >= 0) atomicAdd(&tew[o + idx], wt);
+            count += __popc(newmask);
+            __syncwarp();
+        }
+        if (lane == 0) cnt[c] = count;
+        __syncwarp();
+    }
+}
+
+// one CTA per row of list2 (hubs): table in the global region toff; phase 1
+// inserts (first position by atomicMin, weights by atomicAdd), phase 2 ranks
+// first positions with a block scan in row order.
 __global__ void __launch_bounds__(BIG_T) k_contract_big(DGraph g, const int32_t* __restrict__ list, int64_t nbig,
                                                         const int32_t* __restrict__ mem, const int32_t* __restrict__ cmap,
                                                         const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
                                                         const int64_t* __restrict__ toff, int32_t* __restrict__ gtab,
                                                         int32_t* __restrict__ tci, int32_t* __restrict__ tew,
                                                         int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
-    extern __shared__ int32_t stab[];
     __shared__ int32_t sh[33];
     for (int64_t li = blockIdx.x; li < nbig; li += gridDim.x) {
         const int64_t c = list[li];
@@ -408,7 +481,7 @@ __global__ void __launch_bounds__(BIG_T) k_contract_big(DGraph g, const int32_t*
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        int32_t* keys = S <= SMEM_SLOTS ? stab : gtab + 3 * toff[li];
+        int32_t* keys = gtab + 3 * toff[li];
         int32_t* minpos = keys + S;
         int32_t* wsum = minpos + S;
         for (int64_t i = threadIdx.x; i < S; i += BIG_T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
@@ -492,26 +565,34 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int32_t* tci = c.tmp_alloc<int32_t>(T);
     int32_t* tew = c.tmp_alloc<int32_t>(T);
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
-    int32_t* blist = c.tmp_alloc<int32_t>(nc);
+    int32_t* list1 = c.tmp_alloc<int32_t>(nc);
+    int32_t* list2 = c.tmp_alloc<int32_t>(nc);
     int64_t* tsize = c.tmp_alloc<int64_t>(nc + 1);
     int32_t* err = c.tmp_alloc<int32_t>(1);
-    memset_async(c, d_tot + 1, 0, sizeof(int64_t));
+    memset_async(c, d_tot + 1, 0, 2 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     k_contract_small<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(g, nc, mem, fine.cmap, off, cdeg, tci,
                                                                              tew, rowcnt);
     GP_LAUNCHED(c);
-    k_big_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, blist, tsize, d_tot + 1);
+    k_big_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, list1, list2, tsize, d_tot + 1);
     GP_LAUNCHED(c);
-    const int64_t nbig = read_i64(c, d_tot + 1);
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_tot + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    c.sync();
+    const int64_t nmid = c.h_pinned[0], nbig = c.h_pinned[1];
+    if (nmid > 0) {
+        const int blocks = grid_for(nmid * 32, 256, c.sm_count * 8);
+        const int64_t warps = (int64_t)blocks * 8;
+        int32_t* wtab = c.tmp_alloc<int32_t>(warps * 2 * MID_SLOTS);
+        k_contract_mid<<<blocks, 256, 0, c.s>>>(g, list1, nmid, mem, fine.cmap, off, cdeg, wtab, tci, tew, rowcnt, err);
+        GP_LAUNCHED(c);
+    }
     if (nbig > 0) {
         int64_t* toff = c.tmp_alloc<int64_t>(nbig + 1);
         scan_excl_i64(c, tsize, toff, nbig, toff + nbig);
         const int64_t tslots = read_i64(c, toff + nbig);
         int32_t* gtab = c.tmp_alloc<int32_t>(3 * std::max<int64_t>(tslots, 1));
-        const size_t smem = 3 * sizeof(int32_t) * SMEM_SLOTS;
-        GP_CUDA(cudaFuncSetAttribute(k_contract_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_contract_big<<<(unsigned)std::min<int64_t>(nbig, (int64_t)c.sm_count * 4), BIG_T, smem, c.s>>>(
-            g, blist, nbig, mem, fine.cmap, off, cdeg, toff, gtab, tci, tew, rowcnt, err);
+        k_contract_big<<<(unsigned)std::min<int64_t>(nbig, (int64_t)c.sm_count * 2), BIG_T, 0, c.s>>>(
+            g, list2, nbig, mem, fine.cmap, off, cdeg, toff, gtab, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);
