@@ -270,89 +270,140 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // order; position j in that walk.  Every coarse neighbour is kept once, at
 // the rank of its first position, with the weights of all its positions
 // summed; c itself is dropped.
-constexpr int SMALL_ROW = 128;          // rows up to this length: one warp, 256-slot table on chip
-constexpr int SMALL_SLOTS = 256;
-constexpr int MID_ROW = 8192;           // rows up to this length: one warp, private table in global memory
-constexpr int MID_SLOTS = 2 * MID_ROW;
-constexpr int BIG_T = 1024;             // longer rows: one CTA each, two-phase
+//
+// k_fill_mapped first streams every fine row, mapped through cmap, into the
+// walk layout (row c at off[c]); the dedup kernels then read that buffer
+// coalesced.  Tiers by row length d:
+//   A  d <= 128        one warp, 256-slot table in shared memory
+//   B  d <= 1024       one warp, 2048-slot table in shared memory
+//   C  d <= 4096       one CTA, two-phase (first position by atomicMin), table on chip
+//   D  longer          one CTA, two-phase, table in global memory
+// A and B insert 32 entries at a time in walk order (match_any leaders), so
+// new neighbours get consecutive ranks; C and D rank first positions with one
+// block scan over per-thread contiguous segments.
+constexpr int TA_ROW = 128, TA_SLOTS = 256;
+constexpr int TB_ROW = 1024, TB_SLOTS = 2048, TB_WARPS = 4;
+constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 256;
+constexpr int TD_T = 1024;
 constexpr int32_t EMPTY_KEY = -1;
 
 __device__ __forceinline__ uint32_t slot_hash(int32_t key, int lg) {
     return ((uint32_t)key * 0x9E3779B1u) >> (32 - lg);
 }
 
-__device__ __forceinline__ void row_entry(const DGraph& g, int32_t a, int32_t b, int64_t da, int64_t j,
-                                          const int32_t* __restrict__ cmap, int32_t& cu, int32_t& w) {
-    const int64_t e = j < da ? g.rp[a] + j : g.rp[b] + (j - da);
-    cu = cmap[g.ci[e]];
-    w = g.ew ? g.ew[e] : 1;
+// warp per fine row (CTA per heavy fine row): mapped ids and weights in walk order
+__global__ void __launch_bounds__(256) k_fill_mapped(DGraph g, const int32_t* __restrict__ heavy, int64_t nheavy,
+                                                     const int32_t* __restrict__ cmap, const int32_t* __restrict__ mem,
+                                                     const int64_t* __restrict__ off, int32_t* __restrict__ mapped,
+                                                     int32_t* __restrict__ mw) {
+    auto fill_row = [&](int64_t x, int start, int stride) {
+        const int32_t cc = cmap[x];
+        const int32_t a = mem[2 * (int64_t)cc];
+        const int64_t base = off[cc] + ((int32_t)x == a ? 0 : g.rp[a + 1] - g.rp[a]);
+        const int64_t beg = g.rp[x], end = g.rp[x + 1];
+        for (int64_t e = beg + start; e < end; e += stride) {
+            mapped[base + (e - beg)] = cmap[g.ci[e]];
+            mw[base + (e - beg)] = g.ew ? g.ew[e] : 1;
+        }
+    };
+    if ((int64_t)blockIdx.x < nheavy) {
+        fill_row(heavy[blockIdx.x], threadIdx.x, blockDim.x);
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)(gridDim.x - nheavy) * blockDim.x) >> 5;
+    for (int64_t x = wid; x < g.n; x += nw) {
+        if (g.rp[x + 1] - g.rp[x] > kHeavyDeg) continue;
+        fill_row(x, lane, 32);
+    }
 }
 
-// one warp per coarse row with at most SMALL_ROW entries; table in shared memory
-__global__ void __launch_bounds__(256) k_contract_small(DGraph g, int64_t nc, const int32_t* __restrict__ mem,
-                                                        const int32_t* __restrict__ cmap, const int64_t* __restrict__ off,
-                                                        const int64_t* __restrict__ cdeg, int32_t* __restrict__ tci,
-                                                        int32_t* __restrict__ tew, int32_t* __restrict__ cnt) {
-    __shared__ int32_t s_key[8][SMALL_SLOTS];
-    __shared__ int32_t s_idx[8][SMALL_SLOTS];
-    __shared__ int32_t s_okey[8][SMALL_ROW];
-    __shared__ int32_t s_w[8][SMALL_ROW];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int32_t* key = s_key[w];
-    int32_t* tidx = s_idx[w];
-    int32_t* okey = s_okey[w];
-    int32_t* wacc = s_w[w];
-    for (int i = lane; i < SMALL_SLOTS; i += 32) key[i] = EMPTY_KEY;
-    for (int i = lane; i < SMALL_ROW; i += 32) wacc[i] = 0;
-    __syncwarp();
+// Ordered insertion of one walk by one warp into a shared-memory table.
+// okey/wacc: output ids and weights by rank (shared); returns the row length.
+template <int SLOTS, class IdxT>
+__device__ __forceinline__ int32_t warp_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
+                                              int64_t o, int64_t deg, int32_t self, int32_t* key, IdxT* tidx,
+                                              int32_t* okey, int32_t* wacc, int lg) {
+    const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
+    int32_t count = 0;
+    int32_t cu_next = -1, w_next = 0;
+    if (lane < deg) { cu_next = mapped[o + lane]; w_next = mw[o + lane]; }
+    for (int64_t base = 0; base < deg; base += 32) {
+        const int64_t j = base + lane;
+        const int32_t cu = cu_next, wt = w_next;
+        // prefetch the next chunk
+        if (j + 32 < deg) { cu_next = mapped[o + j + 32]; w_next = mw[o + j + 32]; }
+        const bool act = (j < deg) && cu != self;
+        const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
+        const int leader = __ffs(peers) - 1;
+        bool isnew = false;
+        int32_t h = -1;
+        if (act && lane == leader) {
+            h = (int32_t)slot_hash(cu, lg);
+            for (int probe = 0; probe < SLOTS; ++probe) {
+                const int32_t old = atomicCAS(&key[h], EMPTY_KEY, cu);
+                if (old == EMPTY_KEY) { isnew = true; break; }
+                if (old == cu) break;
+                h = (h + 1) & (SLOTS - 1);
+            }
+        }
+        const uint32_t newmask = __ballot_sync(0xffffffffu, isnew);
+        int32_t idx = -1;
+        if (isnew) {
+            idx = count + __popc(newmask & lt);
+            tidx[h] = (IdxT)idx;
+            okey[idx] = cu;
+        }
+        __syncwarp();
+        if (act && lane == leader && !isnew) idx = tidx[h];
+        idx = __shfl_sync(0xffffffffu, idx, leader);
+        if (act) atomicAdd(&wacc[idx], wt);
+        count += __popc(newmask);
+        __syncwarp();
+    }
+    return count;
+}
+
+template <int MAXROW, int SLOTS, class IdxT>
+__host__ __device__ constexpr size_t warp_dedup_smem() {
+    return ((sizeof(int32_t) * (SLOTS + 2 * MAXROW) + sizeof(IdxT) * SLOTS) + 15) & ~(size_t)15;
+}
+
+// tiers A (MAXROW 128) and B (MAXROW 1024): one warp per row
+template <int MAXROW, int SLOTS, int WARPS, class IdxT>
+__global__ void __launch_bounds__(WARPS * 32) k_dedup_warp(int64_t nc, int64_t minrow, const int64_t* __restrict__ off,
+                                                           const int64_t* __restrict__ cdeg,
+                                                           const int32_t* __restrict__ mapped,
+                                                           const int32_t* __restrict__ mw, int32_t* __restrict__ tci,
+                                                           int32_t* __restrict__ tew, int32_t* __restrict__ cnt) {
+    // dynamic shared memory per warp: key[SLOTS] okey[MAXROW] wacc[MAXROW] idx[SLOTS]
+    extern __shared__ int32_t dsm[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const size_t per_warp = warp_dedup_smem<MAXROW, SLOTS, IdxT>() / sizeof(int32_t);
+    int32_t* key = dsm + w * per_warp;
+    int32_t* okey = key + SLOTS;
+    int32_t* wacc = okey + MAXROW;
+    IdxT* tidx = (IdxT*)(wacc + MAXROW);
+    for (int i = lane; i < SLOTS; i += 32) key[i] = EMPTY_KEY;
+    for (int i = lane; i < MAXROW; i += 32) wacc[i] = 0;
+    __syncwarp();
+    int lg = 0;
+    while ((1 << lg) < SLOTS) ++lg;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t c = wid; c < nc; c += nw) {
         const int64_t deg = cdeg[c];
-        if (deg > SMALL_ROW) continue;
-        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
-        const int64_t da = g.rp[a + 1] - g.rp[a];
-        int32_t count = 0;
-        for (int64_t base = 0; base < deg; base += 32) {
-            const int64_t j = base + lane;
-            int32_t cu = -1, wt = 0;
-            if (j < deg) row_entry(g, a, b, da, j, cmap, cu, wt);
-            const bool act = (j < deg) && cu != (int32_t)c;
-            const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
-            const int leader = __ffs(peers) - 1;
-            bool isnew = false;
-            int32_t h = -1;
-            if (act && lane == leader) {
-                h = (int32_t)slot_hash(cu, 8);
-                for (int probe = 0; probe < SMALL_SLOTS; ++probe) {
-                    const int32_t old = atomicCAS(&key[h], EMPTY_KEY, cu);
-                    if (old == EMPTY_KEY) { isnew = true; break; }
-                    if (old == cu) break;
-                    h = (h + 1) & (SMALL_SLOTS - 1);
-                }
-            }
-            const uint32_t newmask = __ballot_sync(0xffffffffu, isnew);
-            int32_t idx = -1;
-            if (isnew) {
-                idx = count + __popc(newmask & lt);
-                tidx[h] = idx;
-                okey[idx] = cu;
-            }
-            __syncwarp();
-            if (act && lane == leader && !isnew) idx = tidx[h];
-            idx = __shfl_sync(0xffffffffu, idx, leader);
-            if (act) atomicAdd(&wacc[idx], wt);
-            count += __popc(newmask);
-            __syncwarp();
-        }
+        if (deg > MAXROW || deg < minrow) continue;
         const int64_t o = off[c];
+        const int32_t count = warp_dedup<SLOTS, IdxT>(mapped, mw, o, deg, (int32_t)c, key, tidx, okey, wacc, lg);
         for (int i = lane; i < count; i += 32) {
             tci[o + i] = okey[i];
             tew[o + i] = wacc[i];
             wacc[i] = 0;
         }
-        for (int i = lane; i < SMALL_SLOTS; i += 32) key[i] = EMPTY_KEY;
+        for (int i = lane; i < SLOTS; i += 32) key[i] = EMPTY_KEY;
         if (lane == 0) cnt[c] = count;
         __syncwarp();
     }
@@ -379,19 +430,18 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
     return r;
 }
 
-// rows of SMALL_ROW < d <= MID_ROW go to list1, longer ones to list2 (with
-// the size of their global table); list order is irrelevant (rows are independent)
-__global__ void k_big_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ list1,
-                           int32_t* __restrict__ list2, int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
+// rows longer than TB_ROW: list (TC_ROW-bounded rows first use the on-chip table)
+__global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC,
+                            int32_t* __restrict__ listD, int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = cdeg[c];
-        if (d <= SMALL_ROW) continue;
-        if (d <= MID_ROW) {
+        if (d <= TB_ROW) continue;
+        if (d <= TC_ROW) {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[0], 1ull);
-            list1[slot] = (int32_t)c;
+            listC[slot] = (int32_t)c;
         } else {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[1], 1ull);
-            list2[slot] = (int32_t)c;
+            listD[slot] = (int32_t)c;
             int64_t S = 1;
             while (S < 2 * d) S <<= 1;
             tsize[slot] = S;
@@ -399,137 +449,91 @@ __global__ void k_big_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t
     }
 }
 
-// one warp per row of list1, chunks of 32 entries in row order; the table
-// (key, output rank) lives in the warp's private global region (L2 resident),
-// output entries and weights go straight to the temporary row.
-__global__ void __launch_bounds__(256) k_contract_mid(DGraph g, const int32_t* __restrict__ list, int64_t nlist,
-                                                      const int32_t* __restrict__ mem, const int32_t* __restrict__ cmap,
-                                                      const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                      int32_t* __restrict__ wtab, int32_t* __restrict__ tci,
-                                                      int32_t* __restrict__ tew, int32_t* __restrict__ cnt,
-                                                      int32_t* __restrict__ err) {
-    const int lane = threadIdx.x & 31;
-    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    int32_t* key = wtab + wid * (2 * (int64_t)MID_SLOTS);
-    int32_t* tidx = key + MID_SLOTS;
-    const uint32_t lt = (1u << lane) - 1u;
-    for (int64_t li = wid; li < nlist; li += nw) {
+// tiers C and D: one CTA per row, two phases.  Phase 1 inserts every entry
+// (first position by atomicMin, weights by atomicAdd).  Phase 2: each thread
+// owns a contiguous segment of positions, counts the first positions in it,
+// one block scan turns the counts into ranks, and the segment is written.
+template <int T>
+__device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw, int64_t o, int64_t deg,
+                          int32_t self, int32_t* keys, int32_t* minpos, int32_t* wsum, int64_t S, int lg,
+                          int32_t* __restrict__ tci, int32_t* __restrict__ tew, int32_t* cnt_out, int32_t* sh,
+                          int32_t* err) {
+    for (int64_t i = threadIdx.x; i < S; i += T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
+    __syncthreads();
+    for (int64_t j = threadIdx.x; j < deg; j += T) {
+        const int32_t cu = mapped[o + j];
+        if (cu == self) continue;
+        uint32_t h = slot_hash(cu, lg);
+        bool placed = false;
+        for (int64_t probe = 0; probe < S; ++probe) {
+            const int32_t old = atomicCAS(&keys[h], EMPTY_KEY, cu);
+            if (old == EMPTY_KEY || old == cu) { placed = true; break; }
+            h = (h + 1) & (uint32_t)(S - 1);
+        }
+        if (!placed) { atomicExch(err, 1); continue; }
+        atomicMin(&minpos[h], (int32_t)j);
+        atomicAdd(&wsum[h], mw[o + j]);
+    }
+    __syncthreads();
+    const int64_t seg = (deg + T - 1) / T;
+    const int64_t j0 = (int64_t)threadIdx.x * seg, j1 = j0 + seg < deg ? j0 + seg : deg;
+    int32_t mine = 0;
+    for (int64_t j = j0; j < j1; ++j) {
+        const int32_t cu = mapped[o + j];
+        if (cu == self) continue;
+        uint32_t h = slot_hash(cu, lg);
+        for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
+        mine += (minpos[h] == (int32_t)j);
+    }
+    int32_t tot;
+    int32_t r = block_scan_excl(mine, sh, tot);
+    for (int64_t j = j0; j < j1 && mine > 0; ++j) {
+        const int32_t cu = mapped[o + j];
+        if (cu == self) continue;
+        uint32_t h = slot_hash(cu, lg);
+        for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
+        if (minpos[h] == (int32_t)j) { tci[o + r] = cu; tew[o + r] = wsum[h]; ++r; --mine; }
+    }
+    if (threadIdx.x == 0) *cnt_out = tot;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restrict__ list, int64_t nlist,
+                                                         const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
+                                                         const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
+                                                         int32_t* __restrict__ tci, int32_t* __restrict__ tew,
+                                                         int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+    extern __shared__ int32_t stab[];
+    __shared__ int32_t sh[33];
+    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int64_t c = list[li];
         const int64_t deg = cdeg[c];
-        int S = 1, lg = 0;
+        int64_t S = 1;
+        int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        for (int i = lane; i < S; i += 32) key[i] = EMPTY_KEY;
-        __syncwarp();
-        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
-        const int64_t da = g.rp[a + 1] - g.rp[a];
-        const int64_t o = off[c];
-        int32_t count = 0;
-        for (int64_t base = 0; base < deg; base += 32) {
-            const int64_t j = base + lane;
-            int32_t cu = -1, wt = 0;
-            if (j < deg) row_entry(g, a, b, da, j, cmap, cu, wt);
-            const bool act = (j < deg) && cu != (int32_t)c;
-            const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
-            const int leader = __ffs(peers) - 1;
-            bool isnew = false;
-            int32_t h = -1;
-            if (act && lane == leader) {
-                h = (int32_t)slot_hash(cu, lg);
-                bool placed = false;
-                for (int probe = 0; probe < S; ++probe) {
-                    const int32_t old = atomicCAS(&key[h], EMPTY_KEY, cu);
-                    if (old == EMPTY_KEY) { isnew = true; placed = true; break; }
-                    if (old == cu) { placed = true; break; }
-                    h = (h + 1) & (S - 1);
-                }
-                if (!placed) atomicExch(err, 1);
-            }
-            const uint32_t newmask = __ballot_sync(0xffffffffu, isnew);
-            int32_t idx = -1;
-            if (isnew) {
-                idx = count + __popc(newmask & lt);
-                tidx[h] = idx;
-                tci[o + idx] = cu;
-                tew[o + idx] = 0;
-            }
-            __syncwarp();
-            if (act && lane == leader && !isnew && h >= 0) idx = tidx[h];
-            idx = __shfl_sync(0xffffffffu, idx, leader);
-            if (act && idx >= 0) atomicAdd(&tew[o + idx], wt);
-            count += __popc(newmask);
-            __syncwarp();
-        }
-        if (lane == 0) cnt[c] = count;
-        __syncwarp();
+        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, stab, stab + S, stab + 2 * S, S, lg, tci, tew, &cnt[c], sh, err);
     }
 }
 
-// one CTA per row of list2 (hubs): table in the global region toff; phase 1
-// inserts (first position by atomicMin, weights by atomicAdd), phase 2 ranks
-// first positions with a block scan in row order.
-__global__ void __launch_bounds__(BIG_T) k_contract_big(DGraph g, const int32_t* __restrict__ list, int64_t nbig,
-                                                        const int32_t* __restrict__ mem, const int32_t* __restrict__ cmap,
-                                                        const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                        const int64_t* __restrict__ toff, int32_t* __restrict__ gtab,
-                                                        int32_t* __restrict__ tci, int32_t* __restrict__ tew,
-                                                        int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+__global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __restrict__ list, int64_t nlist,
+                                                           const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
+                                                           const int64_t* __restrict__ toff, int32_t* __restrict__ gtab,
+                                                           const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
+                                                           int32_t* __restrict__ tci, int32_t* __restrict__ tew,
+                                                           int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
     __shared__ int32_t sh[33];
-    for (int64_t li = blockIdx.x; li < nbig; li += gridDim.x) {
+    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int64_t c = list[li];
         const int64_t deg = cdeg[c];
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
         int32_t* keys = gtab + 3 * toff[li];
-        int32_t* minpos = keys + S;
-        int32_t* wsum = minpos + S;
-        for (int64_t i = threadIdx.x; i < S; i += BIG_T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
-        __syncthreads();
-        const int32_t a = mem[2 * c], b = mem[2 * c + 1];
-        const int64_t da = g.rp[a + 1] - g.rp[a];
-        for (int64_t j = threadIdx.x; j < deg; j += BIG_T) {
-            int32_t cu, wt;
-            row_entry(g, a, b, da, j, cmap, cu, wt);
-            if (cu == (int32_t)c) continue;
-            uint32_t h = slot_hash(cu, lg);
-            bool placed = false;
-            for (int64_t probe = 0; probe < S; ++probe) {
-                const int32_t old = atomicCAS(&keys[h], EMPTY_KEY, cu);
-                if (old == EMPTY_KEY || old == cu) { placed = true; break; }
-                h = (h + 1) & (uint32_t)(S - 1);
-            }
-            if (!placed) { atomicExch(err, 1); continue; }
-            atomicMin(&minpos[h], (int32_t)j);
-            atomicAdd(&wsum[h], wt);
-        }
-        __syncthreads();
-        int32_t carry = 0;
-        const int64_t o = off[c];
-        for (int64_t base = 0; base < deg; base += BIG_T) {
-            const int64_t j = base + threadIdx.x;
-            int32_t first = 0, cu = -1;
-            uint32_t h = 0;
-            if (j < deg) {
-                int32_t wt;
-                row_entry(g, a, b, da, j, cmap, cu, wt);
-                if (cu != (int32_t)c) {
-                    h = slot_hash(cu, lg);
-                    for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
-                    first = (keys[h] == cu && minpos[h] == (int32_t)j) ? 1 : 0;
-                }
-            }
-            int32_t tot;
-            const int32_t r = block_scan_excl(first, sh, tot);
-            if (first) { tci[o + carry + r] = cu; tew[o + carry + r] = wsum[h]; }
-            carry += tot;
-        }
-        if (threadIdx.x == 0) cnt[c] = carry;
-        __syncthreads();
+        cta_dedup<TD_T>(mapped, mw, off[c], deg, (int32_t)c, keys, keys + S, keys + 2 * S, S, lg, tci, tew, &cnt[c], sh, err);
     }
 }
 
-// warp per coarse row: temporary (row bound offsets) -> final CSR
+// warp per coarse row: temporary (walk-bound offsets) -> final CSR
 __global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, const int64_t* __restrict__ off,
                                                        const int64_t* __restrict__ crp, const int32_t* __restrict__ tci,
                                                        const int32_t* __restrict__ tew, int32_t* __restrict__ ci,
@@ -562,37 +566,54 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int64_t* off = c.tmp_alloc<int64_t>(nc + 1);
     scan_excl_i64(c, cdeg, off, nc, off + nc);
     const int64_t T = g.m;
+    int32_t* mapped = c.tmp_alloc<int32_t>(T);
+    int32_t* mw = c.tmp_alloc<int32_t>(T);
     int32_t* tci = c.tmp_alloc<int32_t>(T);
     int32_t* tew = c.tmp_alloc<int32_t>(T);
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
-    int32_t* list1 = c.tmp_alloc<int32_t>(nc);
-    int32_t* list2 = c.tmp_alloc<int32_t>(nc);
+    int32_t* listC = c.tmp_alloc<int32_t>(nc);
+    int32_t* listD = c.tmp_alloc<int32_t>(nc);
     int64_t* tsize = c.tmp_alloc<int64_t>(nc + 1);
     int32_t* err = c.tmp_alloc<int32_t>(1);
     memset_async(c, d_tot + 1, 0, 2 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
-    k_contract_small<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(g, nc, mem, fine.cmap, off, cdeg, tci,
-                                                                             tew, rowcnt);
-    GP_LAUNCHED(c);
-    k_big_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, list1, list2, tsize, d_tot + 1);
+    {
+        const int grid = (int)fine.nheavy + grid_for(g.n * 32, 256, c.sm_count * 8);
+        k_fill_mapped<<<grid, 256, 0, c.s>>>(g, fine.heavy, fine.nheavy, fine.cmap, mem, off, mapped, mw);
+        GP_LAUNCHED(c);
+    }
+    {
+        constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
+        constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
+        auto kA = k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>;
+        auto kB = k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>;
+        GP_CUDA(cudaFuncSetAttribute(kA, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
+        GP_CUDA(cudaFuncSetAttribute(kB, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+        kA<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, smA, c.s>>>(nc, 0, off, cdeg, mapped, mw, tci, tew, rowcnt);
+        GP_LAUNCHED(c);
+        kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * 6), TB_WARPS * 32, smB, c.s>>>(nc, TA_ROW + 1, off, cdeg,
+                                                                                        mapped, mw, tci, tew, rowcnt);
+        GP_LAUNCHED(c);
+    }
+    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listD, tsize, d_tot + 1);
     GP_LAUNCHED(c);
     GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_tot + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
     c.sync();
-    const int64_t nmid = c.h_pinned[0], nbig = c.h_pinned[1];
-    if (nmid > 0) {
-        const int blocks = grid_for(nmid * 32, 256, c.sm_count * 8);
-        const int64_t warps = (int64_t)blocks * 8;
-        int32_t* wtab = c.tmp_alloc<int32_t>(warps * 2 * MID_SLOTS);
-        k_contract_mid<<<blocks, 256, 0, c.s>>>(g, list1, nmid, mem, fine.cmap, off, cdeg, wtab, tci, tew, rowcnt, err);
+    const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1];
+    if (nC > 0) {
+        const size_t smem = 3 * sizeof(int32_t) * TC_SLOTS;
+        GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * 2), TC_T, smem, c.s>>>(
+            listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
-    if (nbig > 0) {
-        int64_t* toff = c.tmp_alloc<int64_t>(nbig + 1);
-        scan_excl_i64(c, tsize, toff, nbig, toff + nbig);
-        const int64_t tslots = read_i64(c, toff + nbig);
+    if (nD > 0) {
+        int64_t* toff = c.tmp_alloc<int64_t>(nD + 1);
+        scan_excl_i64(c, tsize, toff, nD, toff + nD);
+        const int64_t tslots = read_i64(c, toff + nD);
         int32_t* gtab = c.tmp_alloc<int32_t>(3 * std::max<int64_t>(tslots, 1));
-        k_contract_big<<<(unsigned)std::min<int64_t>(nbig, (int64_t)c.sm_count * 2), BIG_T, 0, c.s>>>(
-            g, list2, nbig, mem, fine.cmap, off, cdeg, toff, gtab, tci, tew, rowcnt, err);
+        k_dedup_cta_global<<<(unsigned)std::min<int64_t>(nD, (int64_t)c.sm_count * 2), TD_T, 0, c.s>>>(
+            listD, nD, off, cdeg, toff, gtab, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);
