@@ -276,7 +276,7 @@ static void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uin
         B.pw = c.keep_alloc<int64_t>(k);
         B.best_pw = c.keep_alloc<int64_t>(k);
         B.status = c.keep_alloc<int64_t>(S_NSLOTS);
-        B.clist = c.keep_alloc<int32_t>(n0);
+        for (int b = 0; b < 3; ++b) B.clist[b] = c.keep_alloc<int32_t>(n0);
         B.ckeys = c.keep_alloc<uint64_t>(n0);
         B.cvals = c.keep_alloc<int32_t>(n0);
         B.ckeys2 = c.keep_alloc<uint64_t>(n0);

@@ -13,25 +13,48 @@
 
 namespace gp {
 
-// ---------------------------------------------------------------- heavy list
-__global__ void k_heavy_list(const int64_t* __restrict__ rp, int64_t n, int32_t* __restrict__ list,
-                             int64_t* __restrict__ count) {
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        if (rp[v + 1] - rp[v] > kHeavyDeg) {
-            unsigned long long slot = atomicAdd((unsigned long long*)count, 1ull);
-            list[slot] = (int32_t)v;
-        }
+// ---------------------------------------------------------------- degree buckets
+// Lists in any order (each row is processed on its own).  Appends are
+// aggregated per warp: one atomic per warp and bucket.
+__device__ __forceinline__ void warp_append(bool take, int32_t v, int32_t* list, int64_t* count) {
+    const uint32_t m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (take) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+__global__ void k_buckets(const int64_t* __restrict__ rp, int64_t n, int32_t* __restrict__ heavy,
+                          int32_t* __restrict__ b0, int32_t* __restrict__ b1, int32_t* __restrict__ b2,
+                          int64_t* __restrict__ count) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t v = base + threadIdx.x;
+        const int64_t d = v < n ? rp[v + 1] - rp[v] : -1;
+        warp_append(v < n && d <= kTile8, (int32_t)v, b0, &count[0]);
+        warp_append(d > kTile8 && d <= kTile32, (int32_t)v, b1, &count[1]);
+        warp_append(d > kTile32 && d <= kHeavyDeg, (int32_t)v, b2, &count[2]);
+        warp_append(d > kHeavyDeg, (int32_t)v, heavy, &count[3]);
     }
 }
 
 void build_heavy(Ctx& c, Level& L) {
-    int64_t* d_cnt = c.tmp_alloc<int64_t>(1);
-    memset_async(c, d_cnt, 0, sizeof(int64_t));
+    auto mk = c.tmp->save();
+    int64_t* d_cnt = c.tmp_alloc<int64_t>(4);
+    memset_async(c, d_cnt, 0, 4 * sizeof(int64_t));
     L.heavy = c.keep_alloc<int32_t>(std::max<int64_t>(1, L.g.m / kHeavyDeg + 1));
-    k_heavy_list<<<grid_for(L.g.n, 256), 256, 0, c.s>>>(L.g.rp, L.g.n, L.heavy, d_cnt);
+    for (int b = 0; b < 3; ++b) L.bucket[b] = c.keep_alloc<int32_t>(L.g.n);
+    k_buckets<<<grid_for(L.g.n, 256), 256, 0, c.s>>>(L.g.rp, L.g.n, L.heavy, L.bucket[0], L.bucket[1], L.bucket[2],
+                                                     d_cnt);
     GP_LAUNCHED(c);
-    c.bytes += 8 * (L.g.n + 1);
-    L.nheavy = read_i64(c, d_cnt);
+    c.bytes += 8 * (L.g.n + 1) + 4 * L.g.n;
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_cnt, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    c.sync();
+    for (int b = 0; b < 3; ++b) L.nbucket[b] = c.h_pinned[b];
+    L.nheavy = c.h_pinned[3];
+    c.tmp->restore(mk);
 }
 
 // ---------------------------------------------------------------- argmax helpers
@@ -65,85 +88,161 @@ __device__ __forceinline__ void block_argmax(uint64_t& k, int32_t& id, uint64_t*
 // ---------------------------------------------------------------- matching
 // MODE 0: proposal to the best eligible unmatched neighbour (handshake round).
 // MODE 1: anchor = best neighbour over all neighbours (two-hop pairing).
+// Work units as in the connectivity pass: rows of the three degree buckets
+// (4 rows per warp for bucket 0, one per warp otherwise), heavy rows one per
+// CTA in blocks [0, nheavy).
+struct MatchArgs {
+    DGraph g;
+    const int32_t* heavy;
+    int64_t nheavy;
+    const int32_t* list[3];   // rows to process, by degree bucket
+    int64_t nlist[3];
+    const int32_t* match;
+    int32_t* out;             // MODE 0: proposals
+    uint64_t salt;
+    int64_t maxvw;
+    uint64_t* keys;           // MODE 1: (anchor << nbits | v)
+    int64_t* nkeys;
+    int nbits;
+};
+
 template <int MODE>
-__device__ __forceinline__ void scan_best(const DGraph& g, int64_t v, int64_t beg, int64_t end, int64_t stride,
-                                          int64_t start, const int32_t* __restrict__ match,
-                                          uint64_t salt, int64_t maxvw, uint64_t& bk, int32_t& bid) {
-    const int64_t vwv = g.vw ? g.vw[v] : 1;
-    for (int64_t e = beg + start; e < end; e += stride) {
-        const int32_t u = g.ci[e];
-        if (u == v) continue;
-        if (MODE == 0) {
-            if (match[u] != -1) continue;
-            if (vwv + (g.vw ? g.vw[u] : 1) > maxvw) continue;
-        }
-        const int32_t w = g.ew ? g.ew[e] : 1;
-        argmax_merge(bk, bid, edge_key(w, edge_hash(salt, (int32_t)v, u)), u);
+__device__ __forceinline__ bool match_ok(const MatchArgs& A, int64_t v, int32_t u, int64_t vwv) {
+    if (u == (int32_t)v) return false;
+    if (MODE == 0) {
+        if (A.match[u] != -1) return false;
+        if (vwv + (A.g.vw ? A.g.vw[u] : 1) > A.maxvw) return false;
     }
+    return true;
 }
 
-// Light rows: one warp per entry of the worklist `wl` (nullptr: every vertex,
-// wl_n = n); rows longer than kHeavyDeg are skipped there and handled by the
-// first nheavy CTAs, one row each.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_match_scan(DGraph g, const int32_t* __restrict__ heavy, int64_t nheavy,
-                                                    const int32_t* __restrict__ wl, int64_t wl_n,
-                                                    const int32_t* __restrict__ match, int32_t* __restrict__ out,
-                                                    uint64_t salt, int64_t maxvw,
-                                                    uint64_t* __restrict__ list_keys, int64_t* __restrict__ list_cnt,
-                                                    int nbits) {
-    __shared__ uint64_t sk[32];
-    __shared__ int32_t sid[32];
-    auto emit = [&](int64_t v, int32_t best) {
-        if (MODE == 0) {
-            out[v] = best;
-        } else if (best >= 0) {
-            unsigned long long slot = atomicAdd((unsigned long long*)list_cnt, 1ull);
-            list_keys[slot] = ((uint64_t)(uint32_t)best << nbits) | (uint64_t)v;
-        }
-    };
-    if ((int64_t)blockIdx.x < nheavy) {
-        const int64_t v = heavy[blockIdx.x];
-        if (match[v] != -1) { if (MODE == 0 && threadIdx.x == 0) out[v] = -1; return; }
-        uint64_t bk = 0; int32_t bid = -1;
-        scan_best<MODE>(g, v, g.rp[v], g.rp[v + 1], blockDim.x, threadIdx.x, match, salt, maxvw, bk, bid);
-        block_argmax(bk, bid, sk, sid);
-        if (threadIdx.x == 0) emit(v, bid);
+__device__ __forceinline__ void match_emit(const MatchArgs& A, bool valid, int64_t v, int32_t best) {
+    if (MODE == 0) {
+        if (valid) A.out[v] = best;
         return;
     }
+    const bool take = valid && best >= 0;
+    const uint32_t m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
     const int lane = threadIdx.x & 31;
-    const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)(gridDim.x - nheavy) * blockDim.x) >> 5;
-    for (int64_t i = wid; i < wl_n; i += nw) {
-        const int64_t v = wl ? wl[i] : i;
-        const int64_t beg = g.rp[v], end = g.rp[v + 1];
-        if (end - beg > kHeavyDeg) continue;
-        if (match[v] != -1) { if (MODE == 0 && lane == 0) out[v] = -1; continue; }
-        if (MODE == 1 && end == beg) continue;
-        uint64_t bk = 0; int32_t bid = -1;
-        scan_best<MODE>(g, v, beg, end, 32, lane, match, salt, maxvw, bk, bid);
-        warp_argmax(bk, bid);
-        if (lane == 0) emit(v, bid);
+    unsigned long long base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)A.nkeys, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (take) A.keys[base + __popc(m & ((1u << lane) - 1u))] = ((uint64_t)(uint32_t)best << A.nbits) | (uint64_t)v;
+}
+
+template <int MODE, int TILE>
+__device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
+    const int lane = threadIdx.x & 31, tl = lane & (TILE - 1);
+    bool valid = v >= 0;
+    if (valid && A.match[v] != -1) valid = false;  // matched already (round 0 / anchors)
+    uint64_t bk = 0;
+    int32_t bid = -1;
+    if (valid) {
+        const int64_t e = A.g.rp[v] + tl;
+        if (e < A.g.rp[v + 1]) {
+            const int32_t u = A.g.ci[e];
+            const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
+            if (match_ok<MODE>(A, v, u, vwv)) {
+                bk = edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, u));
+                bid = u;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = TILE / 2; o > 0; o >>= 1) {
+        const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
+        const int32_t i2 = __shfl_xor_sync(0xffffffffu, bid, o);
+        argmax_merge(bk, bid, k2, i2);
+    }
+    const bool lead = tl == 0;
+    if (MODE == 0) {
+        if (lead && v >= 0) A.out[v] = valid ? bid : -1;
+    } else {
+        match_emit<MODE>(A, lead && valid, v, bid);
     }
 }
 
-// Mutual proposals become pairs; vertices left unmatched are appended to the
-// next round's worklist (any order: each vertex's proposal is its own).
-__global__ void k_handshake(const int32_t* __restrict__ wl, int64_t wl_n, const int32_t* __restrict__ prop,
-                            int32_t* __restrict__ match, int64_t* __restrict__ pairs,
-                            int32_t* __restrict__ next_wl, int64_t* __restrict__ next_n) {
-    int64_t local = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < wl_n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t v = wl ? wl[i] : i;
-        if (match[v] != -1) continue;
-        const int32_t u = prop[v];
-        if (u >= 0 && prop[u] == (int32_t)v) {
-            match[v] = u;
-            if (v < u) ++local;
-        } else {
-            unsigned long long slot = atomicAdd((unsigned long long*)next_n, 1ull);
-            next_wl[slot] = (int32_t)v;
+template <int MODE>
+__global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
+    __shared__ uint64_t sk[32];
+    __shared__ int32_t sid[32];
+    const int lane = threadIdx.x & 31;
+    if ((int64_t)blockIdx.x < A.nheavy) {
+        const int64_t v = A.heavy[blockIdx.x];
+        if (A.match[v] != -1) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
+        const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
+        uint64_t bk = 0; int32_t bid = -1;
+        for (int64_t e = A.g.rp[v] + threadIdx.x; e < A.g.rp[v + 1]; e += blockDim.x) {
+            const int32_t u = A.g.ci[e];
+            if (match_ok<MODE>(A, v, u, vwv))
+                argmax_merge(bk, bid, edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, u)), u);
         }
+        block_argmax(bk, bid, sk, sid);
+        if (threadIdx.x < 32) match_emit<MODE>(A, threadIdx.x == 0, v, bid);
+        return;
+    }
+    const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * blockDim.x) >> 5;
+    const int64_t U0 = (A.nlist[0] + 3) / 4, U1 = A.nlist[1], U2 = A.nlist[2];
+    for (int64_t u = wid; u < U0 + U1 + U2; u += nw) {
+        if (u < U0) {
+            const int64_t i = u * 4 + (lane >> 3);
+            match_tile<MODE, kTile8>(A, i < A.nlist[0] ? A.list[0][i] : -1);
+        } else if (u < U0 + U1) {
+            match_tile<MODE, kTile32>(A, A.list[1][u - U0]);
+        } else {
+            const int64_t v = A.list[2][u - U0 - U1];
+            const bool valid = A.match[v] == -1;
+            uint64_t bk = 0; int32_t bid = -1;
+            if (valid) {
+                const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
+                for (int64_t e = A.g.rp[v] + lane; e < A.g.rp[v + 1]; e += 32) {
+                    const int32_t uu = A.g.ci[e];
+                    if (match_ok<MODE>(A, v, uu, vwv))
+                        argmax_merge(bk, bid, edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, uu)), uu);
+                }
+            }
+            warp_argmax(bk, bid);
+            if (MODE == 0) { if (lane == 0) A.out[v] = valid ? bid : -1; }
+            else match_emit<MODE>(A, lane == 0 && valid, v, bid);
+        }
+    }
+}
+
+// Mutual proposals become pairs; vertices left unmatched go to the next
+// round's worklists, bucketed by degree (any order: each vertex's proposal is
+// its own).  Heavy vertices are not listed: their CTAs check match[] directly.
+__global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, const int32_t* l1, const int32_t* l2,
+                            int64_t n0, int64_t n1, int64_t n2, const int32_t* __restrict__ heavy, int64_t nheavy,
+                            const int32_t* __restrict__ prop, int32_t* __restrict__ match, int64_t* __restrict__ pairs,
+                            int32_t* nl0, int32_t* nl1, int32_t* nl2, int64_t* next_n) {
+    int64_t local = 0;
+    const int64_t total = n0 + n1 + n2 + nheavy;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        int64_t v = -1;
+        if (i < n0) v = l0[i];
+        else if (i < n0 + n1) v = l1[i - n0];
+        else if (i < n0 + n1 + n2) v = l2[i - n0 - n1];
+        else if (i < total) v = heavy[i - n0 - n1 - n2];
+        bool left = false;
+        int64_t d = 0;
+        if (v >= 0 && match[v] == -1) {
+            const int32_t u = prop[v];
+            if (u >= 0 && prop[u] == (int32_t)v) {
+                match[v] = u;
+                if (v < u) ++local;
+            } else {
+                left = true;
+                d = rp[v + 1] - rp[v];
+            }
+        }
+        warp_append(left && d <= kTile8, (int32_t)v, nl0, &next_n[0]);
+        warp_append(left && d > kTile8 && d <= kTile32, (int32_t)v, nl1, &next_n[1]);
+        warp_append(left && d > kTile32 && d <= kHeavyDeg, (int32_t)v, nl2, &next_n[2]);
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
     if ((threadIdx.x & 31) == 0 && local) atomicAdd((unsigned long long*)pairs, (unsigned long long)local);
@@ -182,31 +281,38 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     const uint64_t salt = level_salt(P.seed, level);
     auto mk = c.tmp->save();
     int32_t* prop = c.tmp_alloc<int32_t>(g.n);
-    int32_t* wl[2] = {c.tmp_alloc<int32_t>(g.n), c.tmp_alloc<int32_t>(g.n)};
-    int64_t* d_pairs = c.tmp_alloc<int64_t>(4);
+    int32_t* wl[2][3];
+    for (int s2 = 0; s2 < 2; ++s2)
+        for (int b = 0; b < 3; ++b) wl[s2][b] = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nbucket[b], 1));
+    int64_t* d_cnt = c.tmp_alloc<int64_t>(8);
     GP_CUDA(cudaMemsetAsync(match, 0xff, sizeof(int32_t) * g.n, c.s));
-    const int light_blocks = grid_for(g.n * 32, 256, c.sm_count * 8);
-    const int grid = (int)L.nheavy + light_blocks;
+    MatchArgs A;
+    A.g = g; A.heavy = L.heavy; A.nheavy = L.nheavy; A.match = match; A.out = prop; A.salt = salt;
+    A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0;
+    for (int b = 0; b < 3; ++b) { A.list[b] = L.bucket[b]; A.nlist[b] = L.nbucket[b]; }
     int64_t pairs = 0;
     int rounds = 0;
-    const int32_t* cur = nullptr;   // round 0: every vertex
-    int64_t cur_n = g.n;
-    for (int r = 0; r < P.o.match_rounds && cur_n > 0; ++r) {
-        int32_t* next = wl[r & 1];
-        memset_async(c, d_pairs, 0, 2 * sizeof(int64_t));
-        k_match_scan<0><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, cur, cur_n, match, prop, salt, P.maxvw,
-                                               nullptr, nullptr, 0);
+    for (int r = 0; r < P.o.match_rounds; ++r) {
+        const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
+        if (units == 0 && L.nheavy == 0) break;
+        const int grid = (int)L.nheavy + grid_for(units * 32, 256, c.sm_count * 8);
+        memset_async(c, d_cnt, 0, 4 * sizeof(int64_t));
+        k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);
-        k_handshake<<<grid_for(cur_n, 256), 256, 0, c.s>>>(cur, cur_n, prop, match, d_pairs, next, d_pairs + 1);
+        int32_t** nxt = wl[r & 1];
+        const int64_t tot = A.nlist[0] + A.nlist[1] + A.nlist[2] + L.nheavy;
+        k_handshake<<<grid_for(tot, 256), 256, 0, c.s>>>(g.rp, A.list[0], A.list[1], A.list[2], A.nlist[0], A.nlist[1],
+                                                         A.nlist[2], L.heavy, L.nheavy, prop, match, d_cnt, nxt[0],
+                                                         nxt[1], nxt[2], d_cnt + 1);
         GP_LAUNCHED(c);
-        c.bytes += (L.scan_bytes() + 4 * g.m) * cur_n / std::max<int64_t>(g.n, 1) + 16 * cur_n;
-        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_pairs, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+        const int64_t share = g.n ? (tot * 1000) / g.n : 0;
+        c.bytes += (L.scan_bytes() + 4 * g.m) * share / 1000 + 16 * tot;
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_cnt, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
         c.sync();
         const int64_t newp = c.h_pinned[0];
         rounds = r + 1;
         pairs += newp;
-        cur = next;
-        cur_n = c.h_pinned[1];
+        for (int b = 0; b < 3; ++b) { A.list[b] = nxt[b]; A.nlist[b] = c.h_pinned[1 + b]; }
         if (newp == 0) break;
     }
     if (P.o.two_hop > 0 && 4 * (g.n - pairs) > 3 * g.n) {
@@ -215,19 +321,23 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         uint64_t* keys2 = c.tmp_alloc<uint64_t>(g.n);
         int32_t* vals = c.tmp_alloc<int32_t>(g.n);
         int32_t* vals2 = c.tmp_alloc<int32_t>(g.n);
-        memset_async(c, d_pairs, 0, 2 * sizeof(int64_t));
-        k_match_scan<1><<<grid, 256, 0, c.s>>>(g, L.heavy, L.nheavy, nullptr, g.n, match, nullptr, salt, P.maxvw,
-                                               keys, d_pairs + 1, nb);
+        memset_async(c, d_cnt, 0, 2 * sizeof(int64_t));
+        MatchArgs B2 = A;
+        for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
+        B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
+        const int64_t units = (B2.nlist[0] + 3) / 4 + B2.nlist[1] + B2.nlist[2];
+        const int grid = (int)L.nheavy + grid_for(units * 32, 256, c.sm_count * 8);
+        k_match_scan<1><<<grid, 256, 0, c.s>>>(B2);
         GP_LAUNCHED(c);
         c.bytes += L.scan_bytes() + 4 * g.n;
-        int64_t cnt = read_i64(c, d_pairs + 1);
+        int64_t cnt = read_i64(c, d_cnt + 1);
         if (cnt > 1) {
             GP_CUDA(cudaMemsetAsync(vals, 0, sizeof(int32_t) * cnt, c.s));
             radix_sort_pairs(c, keys, vals, keys2, vals2, cnt, 2 * nb);
-            k_twohop_pair<<<grid_for(cnt, 256), 256, 0, c.s>>>(keys, cnt, nb, g.vw, P.maxvw, match, d_pairs);
+            k_twohop_pair<<<grid_for(cnt, 256), 256, 0, c.s>>>(keys, cnt, nb, g.vw, P.maxvw, match, d_cnt);
             GP_LAUNCHED(c);
             c.bytes += 24 * cnt;
-            pairs += read_i64(c, d_pairs);
+            pairs += read_i64(c, d_cnt);
         }
     }
     c.tmp->restore(mk);
@@ -431,8 +541,9 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
 }
 
 // rows longer than TB_ROW: list (TC_ROW-bounded rows first use the on-chip table)
+// count[0] = rows of tier C, count[1] = rows of tier D, count[2] = longest tier-D row
 __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC,
-                            int32_t* __restrict__ listD, int64_t* __restrict__ tsize, int64_t* __restrict__ count) {
+                            int32_t* __restrict__ listD, int64_t* __restrict__ count) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = cdeg[c];
         if (d <= TB_ROW) continue;
@@ -442,9 +553,7 @@ __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_
         } else {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[1], 1ull);
             listD[slot] = (int32_t)c;
-            int64_t S = 1;
-            while (S < 2 * d) S <<= 1;
-            tsize[slot] = S;
+            atomicMax((unsigned long long*)&count[2], (unsigned long long)d);
         }
     }
 }
@@ -515,9 +624,11 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
     }
 }
 
+// tier D: each CTA owns a table region of region_slots slots (sized for the
+// longest row) and reuses it row after row; few CTAs keep the working set in L2
 __global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __restrict__ list, int64_t nlist,
                                                            const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                           const int64_t* __restrict__ toff, int32_t* __restrict__ gtab,
+                                                           int64_t region_slots, int32_t* __restrict__ gtab,
                                                            const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
                                                            int32_t* __restrict__ tci, int32_t* __restrict__ tew,
                                                            int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
@@ -528,7 +639,7 @@ __global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __rest
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        int32_t* keys = gtab + 3 * toff[li];
+        int32_t* keys = gtab + 3 * region_slots * (int64_t)blockIdx.x;
         cta_dedup<TD_T>(mapped, mw, off[c], deg, (int32_t)c, keys, keys + S, keys + 2 * S, S, lg, tci, tew, &cnt[c], sh, err);
     }
 }
@@ -573,9 +684,9 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
     int32_t* listC = c.tmp_alloc<int32_t>(nc);
     int32_t* listD = c.tmp_alloc<int32_t>(nc);
-    int64_t* tsize = c.tmp_alloc<int64_t>(nc + 1);
+    int64_t* lcount = c.tmp_alloc<int64_t>(3);
     int32_t* err = c.tmp_alloc<int32_t>(1);
-    memset_async(c, d_tot + 1, 0, 2 * sizeof(int64_t));
+    memset_async(c, lcount, 0, 3 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
         const int grid = (int)fine.nheavy + grid_for(g.n * 32, 256, c.sm_count * 8);
@@ -595,11 +706,11 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
                                                                                         mapped, mw, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
-    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listD, tsize, d_tot + 1);
+    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listD, lcount);
     GP_LAUNCHED(c);
-    GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_tot + 1, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
     c.sync();
-    const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1];
+    const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
     if (nC > 0) {
         const size_t smem = 3 * sizeof(int32_t) * TC_SLOTS;
         GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -608,12 +719,12 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         GP_LAUNCHED(c);
     }
     if (nD > 0) {
-        int64_t* toff = c.tmp_alloc<int64_t>(nD + 1);
-        scan_excl_i64(c, tsize, toff, nD, toff + nD);
-        const int64_t tslots = read_i64(c, toff + nD);
-        int32_t* gtab = c.tmp_alloc<int32_t>(3 * std::max<int64_t>(tslots, 1));
-        k_dedup_cta_global<<<(unsigned)std::min<int64_t>(nD, (int64_t)c.sm_count * 2), TD_T, 0, c.s>>>(
-            listD, nD, off, cdeg, toff, gtab, mapped, mw, tci, tew, rowcnt, err);
+        int64_t S = 1;
+        while (S < 2 * maxD) S <<= 1;
+        const int64_t ctas = std::min<int64_t>(nD, 96);
+        int32_t* gtab = c.tmp_alloc<int32_t>(3 * S * ctas);
+        k_dedup_cta_global<<<(unsigned)ctas, TD_T, 0, c.s>>>(listD, nD, off, cdeg, S, gtab, mapped, mw, tci, tew,
+                                                             rowcnt, err);
         GP_LAUNCHED(c);
     }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);

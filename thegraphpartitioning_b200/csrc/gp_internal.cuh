@@ -19,11 +19,20 @@ struct Params {
     gp_options o{};
 };
 
+// Degree classes of the rows of one level; every kernel that works row by
+// row (matching, connectivity, afterburner) schedules its units from these
+// lists: bucket 0 rows go 4 to a warp (8 lanes each), bucket 1 rows one to a
+// warp in registers, bucket 2 rows one to a warp with a shared-memory
+// histogram, heavy rows one to a CTA.
+constexpr int kTile8 = 8;         // bucket 0: degree <= 8
+constexpr int kTile32 = 32;       // bucket 1: degree <= 32
 struct Level {
     DGraph g;
     int32_t* cmap = nullptr;      // fine -> coarse map to the next coarser level
     int32_t* heavy = nullptr;     // vertices with degree > kHeavyDeg
     int64_t nheavy = 0;
+    int32_t* bucket[3] = {nullptr, nullptr, nullptr};
+    int64_t nbucket[3] = {0, 0, 0};
     // bytes of one neighbour scan: row pointers, column ids, weights, gathered per-neighbour int32 state
     int64_t scan_bytes() const { return 8 * (g.n + 1) + 4 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.m; }
 };
@@ -72,7 +81,7 @@ struct RefineBufs {
     int64_t* pw = nullptr;        // k
     int64_t* best_pw = nullptr;   // k
     int64_t* status = nullptr;    // 16
-    int32_t* clist = nullptr;     // LP candidates (light rows)
+    int32_t* clist[3] = {nullptr, nullptr, nullptr};   // LP candidates by degree bucket
     uint64_t* ckeys = nullptr;    // rebalance candidate keys
     int32_t* cvals = nullptr;
     uint64_t* ckeys2 = nullptr;
@@ -81,7 +90,7 @@ struct RefineBufs {
 
 // device status block of the refinement loop; slots [0, S_NRESET) are cleared
 // before every connectivity pass, S_STEP_MOVES before every move step
-enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NCAND = 3, S_LIGHT = 5, S_NLIST = 6, S_CDEG = 7,
+enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NL0 = 3, S_NL1 = 4, S_LIGHT = 5, S_NL2 = 6, S_CDEG = 7,
                   S_NRESET = 8, S_STEP_MOVES = 8, S_NSLOTS = 16 };
 
 // gp_coarsen.cu

@@ -56,16 +56,182 @@ __device__ __forceinline__ bool lp_candidate(int64_t g, int64_t own, int32_t den
 }
 
 // ------------------------------------------------------------------ k_conn
-// status: [S_CROSS] += directed cross weight, [S_MAXPW], [S_MODE], [S_LIGHT] written by CTA 0,
-// [S_NLIST] LP candidates appended to clist (any order: each is evaluated on its own).
-// Rebalance candidates are the vertices with dest >= 0; they are compacted in
-// vertex order afterwards (k_rb_flags + scan + k_rb_compact).
-__global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, int32_t den, int force_eval,
-                                             const int32_t* __restrict__ part, const uint8_t* __restrict__ lock,
-                                             const int64_t* __restrict__ pw, const int32_t* __restrict__ heavy,
-                                             int64_t nheavy, int32_t* __restrict__ dest, int32_t* __restrict__ gain,
-                                             int64_t* __restrict__ status, int32_t* __restrict__ clist) {
+// One unit of work per warp: 4 rows of bucket 0 (8 lanes each), or 1 row of
+// bucket 1, or 1 row of bucket 2; rows longer than kHeavyDeg take CTAs
+// [0, nheavy).  Buckets 0/1 keep their entries in registers and build the
+// connectivity histogram with match_any + redux.sync (no shared memory);
+// bucket 2 and heavy rows use a shared-memory histogram.
+// status: [S_CROSS] += directed cross weight; [S_MAXPW], [S_MODE], [S_LIGHT]
+// written by CTA 0; LP candidates are appended to clist[bucket] (any order:
+// each is evaluated on its own), with [S_NL0..S_NL2] their counts and
+// [S_CDEG] the sum of their degrees.  Rebalance candidates are the vertices
+// with dest >= 0; they are compacted in vertex order afterwards.
+struct ConnArgs {
+    DGraph g;
+    int32_t k;
+    int64_t Lmax;
+    int32_t den;
+    int force_eval;
+    const int32_t* part;
+    const uint8_t* lock;
+    const int64_t* pw;
+    const int32_t* heavy;
+    int64_t nheavy;
+    const int32_t* bucket[3];
+    int64_t nbucket[3];
+    int32_t* dest;
+    int32_t* gain;
+    int64_t* status;
+    int32_t* clist[3];
+};
+
+// warp-aggregated append of the lanes with take set
+__device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, int64_t* count) {
+    const uint32_t m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (take) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// decision of one row from its best other part (bq, bk), own connectivity
+// and total weighted degree; returns true when an LP candidate is recorded
+__device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool active, int64_t v, int32_t p,
+                                            int64_t tot, int64_t cross, uint64_t bk, int32_t bq, int32_t light) {
+    const int64_t own = tot - cross;
+    int32_t d = -1, gn = 0;
+    bool cand = false;
+    if (mode == MODE_LP) {
+        if (active && bq >= 0) {
+            const int64_t gg = (int64_t)bk - own;
+            if (lp_candidate(gg, own, A.den)) { d = bq; gn = (int32_t)gg; cand = true; }
+        }
+    } else if (mode == MODE_RB && active) {
+        const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
+        d = bq >= 0 ? bq : light;
+        gn = -(int32_t)(own - cd);
+    }
+    A.dest[v] = d;
+    A.gain[v] = gn;
+    return cand;
+}
+
+// rows of at most TILE entries, TILE lanes per row, 32/TILE rows per warp
+template <int TILE>
+__device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
+                                          int list_id, int64_t& acc) {
+    const int lane = threadIdx.x & 31, tl = lane & (TILE - 1), tix = lane / TILE;
+    int64_t beg = 0, end = 0;
+    int32_t p = -1;
+    bool active = false;
+    if (v >= 0) {
+        beg = A.g.rp[v]; end = A.g.rp[v + 1];
+        p = A.part[v];
+        active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
+    }
+    const int64_t e = beg + tl;
+    const bool has = v >= 0 && e < end;
+    int32_t q = -1, w = 0;
+    if (has) { q = A.part[A.g.ci[e]]; w = A.g.ew ? A.g.ew[e] : 1; }
+    int32_t cross = (has && q != p) ? w : 0, tot = w;
+#pragma unroll
+    for (int o = TILE / 2; o > 0; o >>= 1) {
+        cross += __shfl_xor_sync(0xffffffffu, cross, o);
+        tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    const uint32_t key = has ? (((uint32_t)tix << 20) | (uint32_t)q) : (0x80000000u | (uint32_t)lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    const int32_t connq = (int32_t)__reduce_add_sync(peers, (uint32_t)w);
+    const bool lead = has && lane == __ffs(peers) - 1;
+    uint64_t bk = 0;
+    int32_t bq = -1;
+    if (active && lead && q != p && (mode != MODE_RB || !over[q])) { bk = (uint64_t)connq; bq = q; }
+#pragma unroll
+    for (int o = TILE / 2; o > 0; o >>= 1) {
+        const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
+        const int32_t q2 = __shfl_xor_sync(0xffffffffu, bq, o);
+        argmax_q(bk, bq, k2, q2);
+    }
+    bool take = false;
+    if (tl == 0 && v >= 0) {
+        acc += cross;
+        take = conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light);
+        if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
+    }
+    warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))]);
+}
+
+// bucket 2: one row per warp, shared-memory histogram; the first CACHED
+// chunks of the row stay in registers between the three sweeps
+template <int CACHED>
+__device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
+                                          int32_t* hist, int64_t& acc) {
+    const int lane = threadIdx.x & 31;
+    const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
+    const int32_t p = A.part[v];
+    const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
+    int32_t qc[CACHED], wc[CACHED];
+    int32_t uc[CACHED];
+#pragma unroll
+    for (int c = 0; c < CACHED; ++c) {
+        const int64_t e = beg + c * 32 + lane;
+        uc[c] = e < end ? A.g.ci[e] : -1;
+        wc[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+    }
+#pragma unroll
+    for (int c = 0; c < CACHED; ++c) qc[c] = uc[c] >= 0 ? A.part[uc[c]] : -1;
+    int32_t cross = 0, tot = 0;
+#pragma unroll
+    for (int c = 0; c < CACHED; ++c) {
+        if (qc[c] < 0) continue;
+        tot += wc[c];
+        if (qc[c] != p) cross += wc[c];
+        if (active) atomicAdd(&hist[qc[c]], wc[c]);
+    }
+    for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) {
+        const int32_t q = A.part[A.g.ci[e]];
+        const int32_t w = A.g.ew ? A.g.ew[e] : 1;
+        tot += w;
+        if (q != p) cross += w;
+        if (active) atomicAdd(&hist[q], w);
+    }
+    cross = warp_sum(cross);
+    tot = warp_sum(tot);
+    uint64_t bk = 0;
+    int32_t bq = -1;
+    if (active) {
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < CACHED; ++c) {
+            const int32_t q = qc[c];
+            if (q >= 0 && q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+        }
+        for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) {
+            const int32_t q = A.part[A.g.ci[e]];
+            if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+        }
+        warp_argmax_q(bk, bq);
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < CACHED; ++c) if (qc[c] >= 0) hist[qc[c]] = 0;
+        for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) hist[A.part[A.g.ci[e]]] = 0;
+        __syncwarp();
+    }
+    bool take = false;
+    if (lane == 0) {
+        acc += cross;
+        take = conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light);
+        if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
+    }
+    warp_push(take, (int32_t)v, A.clist[2], &A.status[S_NL2]);
+}
+
+__global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
     extern __shared__ int32_t csm[];
+    const int32_t k = A.k;
+    const int64_t Lmax = A.Lmax;
     const int kpad = (k + 15) & ~15;
     uint8_t* over = (uint8_t*)csm;
     int32_t* hist_all = csm + kpad / 4;
@@ -80,7 +246,7 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
     int64_t mx = 0;
     uint64_t lk = 0; int32_t lq = -1;  // argmax of (~pw) == argmin pw
     for (int q = threadIdx.x; q < k; q += RT) {
-        const int64_t x = pw[q];
+        const int64_t x = A.pw[q];
         over[q] = x > Lmax;
         mx = x > mx ? x : mx;
         if (x <= Lmax) argmax_q(lk, lq, ~(uint64_t)x, q);
@@ -99,23 +265,23 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
     __syncthreads();
     const int64_t maxpw = s_maxpw;
     const int32_t light = s_light;
-    const int mode = force_eval ? MODE_EVAL : (maxpw > Lmax ? MODE_RB : MODE_LP);
+    const int mode = A.force_eval ? MODE_EVAL : (maxpw > Lmax ? MODE_RB : MODE_LP);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        status[S_MAXPW] = maxpw; status[S_MODE] = mode; status[S_LIGHT] = light;
+        A.status[S_MAXPW] = maxpw; A.status[S_MODE] = mode; A.status[S_LIGHT] = light;
     }
     int64_t acc = 0;  // directed cross weight (this thread)
 
-    if ((int64_t)blockIdx.x < nheavy) {
+    if ((int64_t)blockIdx.x < A.nheavy) {
         // ---- one long row per CTA
         int32_t* hist = hist_all;
-        const int64_t v = heavy[blockIdx.x];
-        const int32_t p = part[v];
-        const bool active = (mode == MODE_LP && !lock[v]) || (mode == MODE_RB && over[p]);
-        const int64_t beg = g.rp[v], end = g.rp[v + 1];
+        const int64_t v = A.heavy[blockIdx.x];
+        const int32_t p = A.part[v];
+        const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
+        const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
         int64_t cross = 0, tot = 0;
         for (int64_t e = beg + threadIdx.x; e < end; e += RT) {
-            const int32_t q = part[g.ci[e]];
-            const int32_t wt = g.ew ? g.ew[e] : 1;
+            const int32_t q = A.part[A.g.ci[e]];
+            const int32_t wt = A.g.ew ? A.g.ew[e] : 1;
             tot += wt;
             if (q != p) cross += wt;
             if (active) atomicAdd(&hist[q], wt);
@@ -142,74 +308,22 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
         if (threadIdx.x == 0) {
             for (int i = 1; i < RW; ++i) argmax_q(bk, bq, s_k[i], s_q[i]);
             acc += cross;
-            const int64_t own = tot - cross;
-            int32_t d = -1, gn = 0;
-            if (mode == MODE_LP && active && bq >= 0) {
-                const int64_t gg = (int64_t)bk - own;
-                if (lp_candidate(gg, own, den)) {
-                    d = bq; gn = (int32_t)gg;
-                    atomicAdd((unsigned long long*)&status[S_CDEG], (unsigned long long)(end - beg));
-                }
-            } else if (mode == MODE_RB && active) {
-                const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
-                d = bq >= 0 ? bq : light;
-                gn = -(int32_t)(own - cd);
-            }
-            dest[v] = d; gain[v] = gn;
+            if (conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light))
+                atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
         }
     } else {
-        // ---- one row per warp
         int32_t* hist = hist_all + w * k;
-        const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * RT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)(gridDim.x - nheavy) * RT) >> 5;
-        for (int64_t v = wid; v < g.n; v += nw) {
-            const int64_t beg = g.rp[v], end = g.rp[v + 1];
-            if (end - beg > kHeavyDeg) continue;
-            const int32_t p = part[v];
-            const bool active = (mode == MODE_LP && !lock[v]) || (mode == MODE_RB && over[p]);
-            int32_t cross = 0, tot = 0;
-            for (int64_t e = beg + lane; e < end; e += 32) {
-                const int32_t q = part[g.ci[e]];
-                const int32_t wt = g.ew ? g.ew[e] : 1;
-                tot += wt;
-                if (q != p) cross += wt;
-                if (active) atomicAdd(&hist[q], wt);
-            }
-            cross = warp_sum(cross); tot = warp_sum(tot);
-            if (lane == 0) acc += cross;
-            if (!active) {
-                if (lane == 0) { dest[v] = -1; gain[v] = 0; }
-                continue;
-            }
-            __syncwarp();
-            uint64_t bk = 0; int32_t bq = -1;
-            for (int64_t e = beg + lane; e < end; e += 32) {
-                const int32_t q = part[g.ci[e]];
-                if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
-            }
-            warp_argmax_q(bk, bq);
-            __syncwarp();
-            for (int64_t e = beg + lane; e < end; e += 32) hist[part[g.ci[e]]] = 0;
-            __syncwarp();
-            if (lane == 0) {
-                const int64_t own = tot - cross;
-                int32_t d = -1, gn = 0;
-                if (mode == MODE_LP) {
-                    if (bq >= 0) {
-                        const int64_t gg = (int64_t)bk - own;
-                        if (lp_candidate(gg, own, den)) {
-                            d = bq; gn = (int32_t)gg;
-                            unsigned long long slot = atomicAdd((unsigned long long*)&status[S_NLIST], 1ull);
-                            clist[slot] = (int32_t)v;
-                            atomicAdd((unsigned long long*)&status[S_CDEG], (unsigned long long)(end - beg));
-                        }
-                    }
-                } else {
-                    const int64_t cd = bq >= 0 ? (int64_t)bk : 0;
-                    d = bq >= 0 ? bq : light;
-                    gn = -(int32_t)(own - cd);
-                }
-                dest[v] = d; gain[v] = gn;
+        const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * RT) >> 5;
+        const int64_t U0 = (A.nbucket[0] + 3) / 4, U1 = A.nbucket[1], U2 = A.nbucket[2];
+        for (int64_t u = wid; u < U0 + U1 + U2; u += nw) {
+            if (u < U0) {
+                const int64_t i = u * 4 + (lane >> 3);
+                conn_tile<kTile8>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
+            } else if (u < U0 + U1) {
+                conn_tile<kTile32>(A, A.bucket[1][u - U0], mode, over, light, 1, acc);
+            } else {
+                conn_warp<4>(A, A.bucket[2][u - U0 - U1], mode, over, light, hist, acc);
             }
         }
     }
@@ -220,7 +334,7 @@ __global__ void __launch_bounds__(RT) k_conn(DGraph g, int32_t k, int64_t Lmax, 
     if (threadIdx.x == 0) {
         int64_t s = 0;
         for (int i = 0; i < RW; ++i) s += s_red[i];
-        if (s) atomicAdd((unsigned long long*)&status[S_CROSS], (unsigned long long)s);
+        if (s) atomicAdd((unsigned long long*)&A.status[S_CROSS], (unsigned long long)s);
     }
 }
 
@@ -247,64 +361,99 @@ __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v
     return pu == d ? wt : (pu == p ? -wt : 0);
 }
 
-__global__ void __launch_bounds__(RT) k_lp_apply(DGraph g, int32_t k, const int32_t* __restrict__ part,
-                                                 const int32_t* __restrict__ dest, const int32_t* __restrict__ gain,
-                                                 const int32_t* __restrict__ heavy, int64_t nheavy,
-                                                 const int32_t* __restrict__ clist, const int64_t* __restrict__ status,
-                                                 int32_t* __restrict__ part_next, uint8_t* __restrict__ lock_next,
-                                                 int64_t* __restrict__ pw, int64_t* __restrict__ moves_out) {
+struct ApplyArgs {
+    DGraph g;
+    int32_t k;
+    const int32_t* part;
+    const int32_t* dest;
+    const int32_t* gain;
+    const int32_t* heavy;
+    int64_t nheavy;
+    const int32_t* clist[3];
+    const int64_t* status;
+    int32_t* part_next;
+    uint8_t* lock_next;
+    int64_t* pw;
+    int64_t* moves_out;
+};
+
+__device__ __forceinline__ void ab_commit(const ApplyArgs& A, int64_t v, int32_t p, int32_t d, int64_t* delta,
+                                          int64_t& moves) {
+    A.part_next[v] = d;
+    A.lock_next[v] = 1;
+    const int64_t wv = A.g.vw ? A.g.vw[v] : 1;
+    atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
+    atomicAdd((unsigned long long*)&delta[p], (unsigned long long)(-wv));
+    ++moves;
+}
+
+// candidate rows of at most TILE entries, TILE lanes each
+template <int TILE>
+__device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
+    const int lane = threadIdx.x & 31, tl = lane & (TILE - 1);
+    int32_t t = 0, p = -1, d = -1;
+    if (v >= 0) {
+        d = A.dest[v]; p = A.part[v];
+        const int32_t gv = A.gain[v];
+        const int64_t e = A.g.rp[v] + tl;
+        if (e < A.g.rp[v + 1]) t = ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
+    }
+#pragma unroll
+    for (int o = TILE / 2; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (tl == 0 && v >= 0 && t >= 0) ab_commit(A, v, p, d, delta, moves);
+}
+
+__global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
     extern __shared__ int64_t delta[];
     __shared__ int32_t s_red[RW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int q = threadIdx.x; q < k; q += RT) delta[q] = 0;
+    for (int q = threadIdx.x; q < A.k; q += RT) delta[q] = 0;
     __syncthreads();
     int64_t moves = 0;
-    if ((int64_t)blockIdx.x < nheavy) {
-        const int64_t v = heavy[blockIdx.x];
-        const int32_t d = dest[v];
+    if ((int64_t)blockIdx.x < A.nheavy) {
+        const int64_t v = A.heavy[blockIdx.x];
+        const int32_t d = A.dest[v];
         if (d >= 0) {
-            const int32_t p = part[v], gv = gain[v];
+            const int32_t p = A.part[v], gv = A.gain[v];
             int32_t g2 = 0;
-            for (int64_t e = g.rp[v] + threadIdx.x; e < g.rp[v + 1]; e += RT) g2 += ab_term(g, e, v, p, d, gv, part, dest, gain);
+            for (int64_t e = A.g.rp[v] + threadIdx.x; e < A.g.rp[v + 1]; e += RT)
+                g2 += ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
             g2 = warp_sum(g2);
             if (lane == 0) s_red[w] = g2;
             __syncthreads();
             if (threadIdx.x == 0) {
                 int32_t s = 0;
                 for (int i = 0; i < RW; ++i) s += s_red[i];
-                if (s >= 0) {
-                    part_next[v] = d; lock_next[v] = 1;
-                    const int64_t wv = g.vw ? g.vw[v] : 1;
-                    atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
-                    atomicAdd((unsigned long long*)&delta[p], (unsigned long long)(-wv));
-                    moves = 1;
-                }
+                if (s >= 0) ab_commit(A, v, p, d, delta, moves);
             }
         }
     } else {
-        const int64_t ncl = status[S_NLIST];
-        const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * RT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)(gridDim.x - nheavy) * RT) >> 5;
-        for (int64_t i = wid; i < ncl; i += nw) {
-            const int64_t v = clist[i];
-            const int32_t d = dest[v], p = part[v], gv = gain[v];
-            int32_t g2 = 0;
-            for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32) g2 += ab_term(g, e, v, p, d, gv, part, dest, gain);
-            g2 = warp_sum(g2);
-            if (lane == 0 && g2 >= 0) {
-                part_next[v] = d; lock_next[v] = 1;
-                const int64_t wv = g.vw ? g.vw[v] : 1;
-                atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
-                atomicAdd((unsigned long long*)&delta[p], (unsigned long long)(-wv));
-                ++moves;
+        const int64_t n0 = A.status[S_NL0], n1 = A.status[S_NL1], n2 = A.status[S_NL2];
+        const int64_t U0 = (n0 + 3) / 4;
+        const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * RT) >> 5;
+        for (int64_t u = wid; u < U0 + n1 + n2; u += nw) {
+            if (u < U0) {
+                const int64_t i = u * 4 + (lane >> 3);
+                ab_tile<kTile8>(A, i < n0 ? A.clist[0][i] : -1, delta, moves);
+            } else if (u < U0 + n1) {
+                ab_tile<kTile32>(A, A.clist[1][u - U0], delta, moves);
+            } else {
+                const int64_t v = A.clist[2][u - U0 - n1];
+                const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
+                int32_t g2 = 0;
+                for (int64_t e = A.g.rp[v] + lane; e < A.g.rp[v + 1]; e += 32)
+                    g2 += ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
+                g2 = warp_sum(g2);
+                if (lane == 0 && g2 >= 0) ab_commit(A, v, p, d, delta, moves);
             }
         }
     }
     moves = warp_sum(moves);
     __syncthreads();
-    if (lane == 0 && moves) atomicAdd((unsigned long long*)moves_out, (unsigned long long)moves);
-    for (int q = threadIdx.x; q < k; q += RT)
-        if (delta[q]) atomicAdd((unsigned long long*)&pw[q], (unsigned long long)delta[q]);
+    if (lane == 0 && moves) atomicAdd((unsigned long long*)A.moves_out, (unsigned long long)moves);
+    for (int q = threadIdx.x; q < A.k; q += RT)
+        if (delta[q]) atomicAdd((unsigned long long*)&A.pw[q], (unsigned long long)delta[q]);
 }
 
 // ------------------------------------------------------------------ rebalance
@@ -534,8 +683,12 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         const bool final_eval = (it == P.o.refine_max_iters);
         GP_CUDA(cudaMemsetAsync(B.status, 0, sizeof(int64_t) * S_NRESET, c.s));
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_a, c.s));
-        k_conn<<<grid, RT, conn_smem, c.s>>>(g, k, Lmax, P.o.lp_filter_den, final_eval ? 1 : 0, B.part, B.lock, B.pw,
-                                             L.heavy, L.nheavy, B.dest, B.gain, B.status, B.clist);
+        ConnArgs CA;
+        CA.g = g; CA.k = k; CA.Lmax = Lmax; CA.den = P.o.lp_filter_den; CA.force_eval = final_eval ? 1 : 0;
+        CA.part = B.part; CA.lock = B.lock; CA.pw = B.pw; CA.heavy = L.heavy; CA.nheavy = L.nheavy;
+        for (int b = 0; b < 3; ++b) { CA.bucket[b] = L.bucket[b]; CA.nbucket[b] = L.nbucket[b]; CA.clist[b] = B.clist[b]; }
+        CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
+        k_conn<<<grid, RT, conn_smem, c.s>>>(CA);
         GP_LAUNCHED(c);
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_b, c.s));
         // rowptr, colidx, weights, gathered part[u]; part[v], lock[v] read; dest, gain written
@@ -553,7 +706,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         const int64_t cur_cut = c.h_pinned[S_CROSS] / 2;
         const int64_t cur_mp = c.h_pinned[S_MAXPW];
         const int dev_mode = (int)c.h_pinned[S_MODE];
-        const int64_t nlist = c.h_pinned[S_NLIST];
+        const int64_t nlist = c.h_pinned[S_NL0] + c.h_pinned[S_NL1] + c.h_pinned[S_NL2];
         const int64_t cdeg = c.h_pinned[S_CDEG];
         if (it == 0) {
             best_cut = cur_cut; best_mp = cur_mp;
@@ -591,8 +744,13 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         if (mode == 0) {
             k_copy_state<<<grid_for(n, 256), 256, 0, c.s>>>(n, B.part, B.part_next, B.lock_next);
             GP_LAUNCHED(c);
-            k_lp_apply<<<grid, RT, sizeof(int64_t) * k, c.s>>>(g, k, B.part, B.dest, B.gain, L.heavy, L.nheavy, B.clist,
-                                                              B.status, B.part_next, B.lock_next, B.pw, moves_d);
+            ApplyArgs AA;
+            AA.g = g; AA.k = k; AA.part = B.part; AA.dest = B.dest; AA.gain = B.gain; AA.heavy = L.heavy;
+            AA.nheavy = L.nheavy;
+            for (int b = 0; b < 3; ++b) AA.clist[b] = B.clist[b];
+            AA.status = B.status; AA.part_next = B.part_next; AA.lock_next = B.lock_next; AA.pw = B.pw;
+            AA.moves_out = moves_d;
+            k_lp_apply<<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
             GP_LAUNCHED(c);
             // copy pass + afterburner: candidate rows with three gathered int32 per entry
             c.bytes += 9 * n + 16 * nlist + cdeg * (4 + (g.ew ? 4 : 0) + 12);
