@@ -198,10 +198,27 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
             uint64_t bk = 0; int32_t bid = -1;
             if (valid) {
                 const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
-                for (int64_t e = A.g.rp[v] + lane; e < A.g.rp[v + 1]; e += 32) {
-                    const int32_t uu = A.g.ci[e];
-                    if (match_ok<MODE>(A, v, uu, vwv))
-                        argmax_merge(bk, bid, edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, uu)), uu);
+                const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
+                for (int64_t base = beg; base < end; base += 128) {
+                    int32_t uu[4], ww[4], mm[4], vv[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int64_t e = base + c * 32 + lane;
+                        uu[c] = e < end ? A.g.ci[e] : -1;
+                        ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        mm[c] = (MODE == 0 && uu[c] >= 0) ? A.match[uu[c]] : -1;
+                        vv[c] = (MODE == 0 && uu[c] >= 0 && A.g.vw) ? A.g.vw[uu[c]] : 1;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int32_t x = uu[c];
+                        if (x < 0 || x == (int32_t)v) continue;
+                        if (MODE == 0 && (mm[c] != -1 || vwv + vv[c] > A.maxvw)) continue;
+                        argmax_merge(bk, bid, edge_key(ww[c], edge_hash(A.salt, (int32_t)v, x)), x);
+                    }
                 }
             }
             warp_argmax(bk, bid);
@@ -559,49 +576,87 @@ __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_
 }
 
 // tiers C and D: one CTA per row, two phases.  Phase 1 inserts every entry
-// (first position by atomicMin, weights by atomicAdd).  Phase 2: each thread
-// owns a contiguous segment of positions, counts the first positions in it,
-// one block scan turns the counts into ranks, and the segment is written.
+// (first position by atomicMin, weights by atomicAdd), four entries per
+// thread in flight.  Phase 2: warps ballot the first-position flags of 32
+// consecutive positions into one word each, one block scan over the word
+// popcounts gives each word's base rank, and a second strided sweep writes
+// the first occurrences at base + rank within the word.
+// words: 2 * ceil(deg/32) ints of scratch (bits, then prefix).
 template <int T>
 __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw, int64_t o, int64_t deg,
                           int32_t self, int32_t* keys, int32_t* minpos, int32_t* wsum, int64_t S, int lg,
-                          int32_t* __restrict__ tci, int32_t* __restrict__ tew, int32_t* cnt_out, int32_t* sh,
-                          int32_t* err) {
+                          int32_t* words, int32_t* __restrict__ tci, int32_t* __restrict__ tew, int32_t* cnt_out,
+                          int32_t* sh, int32_t* err) {
+    const uint32_t mask = (uint32_t)(S - 1);
     for (int64_t i = threadIdx.x; i < S; i += T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
     __syncthreads();
-    for (int64_t j = threadIdx.x; j < deg; j += T) {
-        const int32_t cu = mapped[o + j];
-        if (cu == self) continue;
-        uint32_t h = slot_hash(cu, lg);
-        bool placed = false;
-        for (int64_t probe = 0; probe < S; ++probe) {
-            const int32_t old = atomicCAS(&keys[h], EMPTY_KEY, cu);
-            if (old == EMPTY_KEY || old == cu) { placed = true; break; }
-            h = (h + 1) & (uint32_t)(S - 1);
+    for (int64_t base = 0; base < deg; base += 4 * T) {
+        int32_t cu[4], wt[4], old[4];
+        uint32_t h[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t j = base + c * T + threadIdx.x;
+            cu[c] = j < deg ? mapped[o + j] : self;
+            wt[c] = j < deg ? mw[o + j] : 0;
         }
-        if (!placed) { atomicExch(err, 1); continue; }
-        atomicMin(&minpos[h], (int32_t)j);
-        atomicAdd(&wsum[h], mw[o + j]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            h[c] = slot_hash(cu[c], lg);
+            old[c] = cu[c] != self ? atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]) : EMPTY_KEY;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (cu[c] == self) continue;
+            int64_t probe = 1;
+            while (old[c] != EMPTY_KEY && old[c] != cu[c] && probe < S) {
+                h[c] = (h[c] + 1) & mask;
+                old[c] = atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]);
+                ++probe;
+            }
+            if (old[c] != EMPTY_KEY && old[c] != cu[c]) { atomicExch(err, 1); continue; }
+            atomicMin(&minpos[h[c]], (int32_t)(base + c * T + threadIdx.x));
+            atomicAdd(&wsum[h[c]], wt[c]);
+        }
     }
     __syncthreads();
-    const int64_t seg = (deg + T - 1) / T;
-    const int64_t j0 = (int64_t)threadIdx.x * seg, j1 = j0 + seg < deg ? j0 + seg : deg;
-    int32_t mine = 0;
-    for (int64_t j = j0; j < j1; ++j) {
-        const int32_t cu = mapped[o + j];
-        if (cu == self) continue;
-        uint32_t h = slot_hash(cu, lg);
-        for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
-        mine += (minpos[h] == (int32_t)j);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = T / 32;
+    const int64_t nwords = (deg + 31) / 32;
+    int32_t* bits = words;
+    int32_t* wpre = words + nwords;
+    auto lookup = [&](int32_t cu) -> uint32_t {
+        uint32_t hh = slot_hash(cu, lg);
+        for (int64_t probe = 0; probe < S && keys[hh] != cu; ++probe) hh = (hh + 1) & mask;
+        return hh;
+    };
+    for (int64_t wi = wid; wi < nwords; wi += nwarp) {
+        const int64_t j = wi * 32 + lane;
+        bool first = false;
+        if (j < deg) {
+            const int32_t cu = mapped[o + j];
+            if (cu != self) first = minpos[lookup(cu)] == (int32_t)j;
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, first);
+        if (lane == 0) bits[wi] = (int32_t)word;
     }
+    __syncthreads();
+    // exclusive scan of word popcounts: contiguous word ranges per thread
+    const int64_t per = (nwords + T - 1) / T;
+    const int64_t w0 = (int64_t)threadIdx.x * per, w1 = w0 + per < nwords ? w0 + per : nwords;
+    int32_t mine = 0;
+    for (int64_t wi = w0; wi < w1; ++wi) mine += __popc((uint32_t)bits[wi]);
     int32_t tot;
-    int32_t r = block_scan_excl(mine, sh, tot);
-    for (int64_t j = j0; j < j1 && mine > 0; ++j) {
+    int32_t run = block_scan_excl(mine, sh, tot);
+    for (int64_t wi = w0; wi < w1; ++wi) { wpre[wi] = run; run += __popc((uint32_t)bits[wi]); }
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int64_t wi = wid; wi < nwords; wi += nwarp) {
+        const uint32_t word = (uint32_t)bits[wi];
+        if (!((word >> lane) & 1u)) continue;
+        const int64_t j = wi * 32 + lane;
         const int32_t cu = mapped[o + j];
-        if (cu == self) continue;
-        uint32_t h = slot_hash(cu, lg);
-        for (int64_t probe = 0; probe < S && keys[h] != cu; ++probe) h = (h + 1) & (uint32_t)(S - 1);
-        if (minpos[h] == (int32_t)j) { tci[o + r] = cu; tew[o + r] = wsum[h]; ++r; --mine; }
+        const int32_t r = wpre[wi] + __popc(word & lt);
+        tci[o + r] = cu;
+        tew[o + r] = wsum[lookup(cu)];
     }
     if (threadIdx.x == 0) *cnt_out = tot;
     __syncthreads();
@@ -620,7 +675,8 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, stab, stab + S, stab + 2 * S, S, lg, tci, tew, &cnt[c], sh, err);
+        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, stab, stab + S, stab + 2 * S, S, lg, stab + 3 * TC_SLOTS,
+                        tci, tew, &cnt[c], sh, err);
     }
 }
 
@@ -628,7 +684,8 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
 // longest row) and reuses it row after row; few CTAs keep the working set in L2
 __global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __restrict__ list, int64_t nlist,
                                                            const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                           int64_t region_slots, int32_t* __restrict__ gtab,
+                                                           int64_t region_slots, int64_t region_ints,
+                                                           int32_t* __restrict__ gtab,
                                                            const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
                                                            int32_t* __restrict__ tci, int32_t* __restrict__ tew,
                                                            int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
@@ -639,8 +696,9 @@ __global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __rest
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        int32_t* keys = gtab + 3 * region_slots * (int64_t)blockIdx.x;
-        cta_dedup<TD_T>(mapped, mw, off[c], deg, (int32_t)c, keys, keys + S, keys + 2 * S, S, lg, tci, tew, &cnt[c], sh, err);
+        int32_t* keys = gtab + region_ints * (int64_t)blockIdx.x;
+        cta_dedup<TD_T>(mapped, mw, off[c], deg, (int32_t)c, keys, keys + S, keys + 2 * S, S, lg, keys + 3 * region_slots,
+                        tci, tew, &cnt[c], sh, err);
     }
 }
 
@@ -712,7 +770,7 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     c.sync();
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
     if (nC > 0) {
-        const size_t smem = 3 * sizeof(int32_t) * TC_SLOTS;
+        const size_t smem = sizeof(int32_t) * (3 * TC_SLOTS + 2 * ((TC_ROW + 31) / 32));
         GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * 2), TC_T, smem, c.s>>>(
             listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
@@ -722,9 +780,10 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         int64_t S = 1;
         while (S < 2 * maxD) S <<= 1;
         const int64_t ctas = std::min<int64_t>(nD, 96);
-        int32_t* gtab = c.tmp_alloc<int32_t>(3 * S * ctas);
-        k_dedup_cta_global<<<(unsigned)ctas, TD_T, 0, c.s>>>(listD, nD, off, cdeg, S, gtab, mapped, mw, tci, tew,
-                                                             rowcnt, err);
+        const int64_t region_ints = 3 * S + 2 * ((maxD + 31) / 32);
+        int32_t* gtab = c.tmp_alloc<int32_t>(region_ints * ctas);
+        k_dedup_cta_global<<<(unsigned)ctas, TD_T, 0, c.s>>>(listD, nD, off, cdeg, S, region_ints, gtab, mapped, mw,
+                                                             tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);

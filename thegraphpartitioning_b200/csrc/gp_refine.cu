@@ -163,39 +163,35 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))]);
 }
 
-// bucket 2: one row per warp, shared-memory histogram; the first CACHED
-// chunks of the row stay in registers between the three sweeps
-template <int CACHED>
+// bucket 2: one row per warp, shared-memory histogram.  The row is swept
+// 128 entries at a time (4 independent loads per lane in flight).  For rows
+// at least as long as k the best part is taken over the k histogram bins,
+// otherwise over the row's entries again (same candidates: parts with a
+// non-zero connection).
 __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
                                           int32_t* hist, int64_t& acc) {
     const int lane = threadIdx.x & 31;
     const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
     const int32_t p = A.part[v];
     const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
-    int32_t qc[CACHED], wc[CACHED];
-    int32_t uc[CACHED];
-#pragma unroll
-    for (int c = 0; c < CACHED; ++c) {
-        const int64_t e = beg + c * 32 + lane;
-        uc[c] = e < end ? A.g.ci[e] : -1;
-        wc[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
-    }
-#pragma unroll
-    for (int c = 0; c < CACHED; ++c) qc[c] = uc[c] >= 0 ? A.part[uc[c]] : -1;
     int32_t cross = 0, tot = 0;
+    for (int64_t base = beg; base < end; base += 128) {
+        int32_t u[4], w[4], q[4];
 #pragma unroll
-    for (int c = 0; c < CACHED; ++c) {
-        if (qc[c] < 0) continue;
-        tot += wc[c];
-        if (qc[c] != p) cross += wc[c];
-        if (active) atomicAdd(&hist[qc[c]], wc[c]);
-    }
-    for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) {
-        const int32_t q = A.part[A.g.ci[e]];
-        const int32_t w = A.g.ew ? A.g.ew[e] : 1;
-        tot += w;
-        if (q != p) cross += w;
-        if (active) atomicAdd(&hist[q], w);
+        for (int c = 0; c < 4; ++c) {
+            const int64_t e = base + c * 32 + lane;
+            u[c] = e < end ? A.g.ci[e] : -1;
+            w[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? A.part[u[c]] : -1;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (q[c] < 0) continue;
+            tot += w[c];
+            if (q[c] != p) cross += w[c];
+            if (active) atomicAdd(&hist[q[c]], w[c]);
+        }
     }
     cross = warp_sum(cross);
     tot = warp_sum(tot);
@@ -203,20 +199,23 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
     int32_t bq = -1;
     if (active) {
         __syncwarp();
-#pragma unroll
-        for (int c = 0; c < CACHED; ++c) {
-            const int32_t q = qc[c];
-            if (q >= 0 && q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+        if (end - beg >= A.k) {
+            for (int q = lane; q < A.k; q += 32) {
+                const int32_t h = hist[q];
+                if (h > 0 && q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)h, q);
+            }
+            warp_argmax_q(bk, bq);
+            __syncwarp();
+            for (int q = lane; q < A.k; q += 32) hist[q] = 0;
+        } else {
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const int32_t q = A.part[A.g.ci[e]];
+                if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+            }
+            warp_argmax_q(bk, bq);
+            __syncwarp();
+            for (int64_t e = beg + lane; e < end; e += 32) hist[A.part[A.g.ci[e]]] = 0;
         }
-        for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) {
-            const int32_t q = A.part[A.g.ci[e]];
-            if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
-        }
-        warp_argmax_q(bk, bq);
-        __syncwarp();
-#pragma unroll
-        for (int c = 0; c < CACHED; ++c) if (qc[c] >= 0) hist[qc[c]] = 0;
-        for (int64_t e = beg + CACHED * 32 + lane; e < end; e += 32) hist[A.part[A.g.ci[e]]] = 0;
         __syncwarp();
     }
     bool take = false;
@@ -279,12 +278,23 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
         const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
         const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
         int64_t cross = 0, tot = 0;
-        for (int64_t e = beg + threadIdx.x; e < end; e += RT) {
-            const int32_t q = A.part[A.g.ci[e]];
-            const int32_t wt = A.g.ew ? A.g.ew[e] : 1;
-            tot += wt;
-            if (q != p) cross += wt;
-            if (active) atomicAdd(&hist[q], wt);
+        for (int64_t base = beg; base < end; base += 4 * RT) {
+            int32_t uu[4], ww[4], qq[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int64_t e = base + c * RT + threadIdx.x;
+                uu[c] = e < end ? A.g.ci[e] : -1;
+                ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (qq[c] < 0) continue;
+                tot += ww[c];
+                if (qq[c] != p) cross += ww[c];
+                if (active) atomicAdd(&hist[qq[c]], ww[c]);
+            }
         }
         cross = warp_sum(cross); tot = warp_sum(tot);
         __syncthreads();
@@ -323,7 +333,7 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
             } else if (u < U0 + U1) {
                 conn_tile<kTile32>(A, A.bucket[1][u - U0], mode, over, light, 1, acc);
             } else {
-                conn_warp<4>(A, A.bucket[2][u - U0 - U1], mode, over, light, hist, acc);
+                conn_warp(A, A.bucket[2][u - U0 - U1], mode, over, light, hist, acc);
             }
         }
     }
@@ -441,9 +451,32 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
             } else {
                 const int64_t v = A.clist[2][u - U0 - n1];
                 const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
+                const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
                 int32_t g2 = 0;
-                for (int64_t e = A.g.rp[v] + lane; e < A.g.rp[v + 1]; e += 32)
-                    g2 += ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
+                for (int64_t base = beg; base < end; base += 128) {
+                    int32_t uu[4], ww[4], pu[4], du[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int64_t e = base + c * 32 + lane;
+                        uu[c] = e < end ? A.g.ci[e] : -1;
+                        ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        pu[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
+                        du[c] = uu[c] >= 0 ? A.dest[uu[c]] : -1;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (uu[c] < 0) continue;
+                        int32_t q = pu[c];
+                        if (du[c] >= 0) {
+                            const int32_t gu = A.gain[uu[c]];
+                            if (gu > gv || (gu == gv && uu[c] < (int32_t)v)) q = du[c];
+                        }
+                        g2 += q == d ? ww[c] : (q == p ? -ww[c] : 0);
+                    }
+                }
                 g2 = warp_sum(g2);
                 if (lane == 0 && g2 >= 0) ab_commit(A, v, p, d, delta, moves);
             }
