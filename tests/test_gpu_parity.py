@@ -24,6 +24,9 @@ def _cases():
     yield "grid3d_k32", graphs.grid3d(16, 16, 16), 32, 0.03, None, {}
     yield "weighted_k5", graphs.grid2d(40, 50), 5, 0.05, "w", {}
     yield "star_heavy_k4", star_plus_grid(), 4, 0.03, None, {"coarsen_to": 200}
+    # a hub of 40000 leaves: rows split over several CTAs, longest contraction tier
+    yield "megahub_k8", star_plus_grid(leaves=40000, side=64), 8, 0.03, None, {}
+    yield "megahub_w_k3", star_plus_grid(leaves=36000, side=40), 3, 0.05, "w", {"coarsen_to": 300}
     yield "rmat11_k64_tight", graphs.rmat(11, seed=3)[:2], 64, 0.0, None, {}
     yield "er_k3_nohop", graphs.erdos_renyi(3000, 3.0, seed=5), 3, 0.02, None, {"two_hop": -1}
     yield "rgg_k2", graphs.random_geometric(4000, 8.0, seed=6), 2, 0.03, None, {"init_trials": 8}

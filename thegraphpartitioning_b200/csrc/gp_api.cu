@@ -277,6 +277,14 @@ static void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uin
         B.best_pw = c.keep_alloc<int64_t>(k);
         B.status = c.keep_alloc<int64_t>(S_NSLOTS);
         for (int b = 0; b < 3; ++b) B.clist[b] = c.keep_alloc<int32_t>(n0);
+        int64_t hmax = 1;
+        for (const Level& l : lv) hmax = std::max(hmax, l.nheavy);
+        B.hhist = c.keep_alloc<int32_t>(hmax * k);
+        B.hsum = c.keep_alloc<int64_t>(2 * hmax);
+        B.hdone = c.keep_alloc<int32_t>(hmax);
+        memset_async(c, B.hhist, 0, sizeof(int32_t) * hmax * k);
+        memset_async(c, B.hsum, 0, sizeof(int64_t) * 2 * hmax);
+        memset_async(c, B.hdone, 0, sizeof(int32_t) * hmax);
         B.ckeys = c.keep_alloc<uint64_t>(n0);
         B.cvals = c.keep_alloc<int32_t>(n0);
         B.ckeys2 = c.keep_alloc<uint64_t>(n0);

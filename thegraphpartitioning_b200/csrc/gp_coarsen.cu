@@ -40,6 +40,14 @@ __global__ void k_buckets(const int64_t* __restrict__ rp, int64_t n, int32_t* __
     }
 }
 
+__global__ void k_heavy_bounds(const int64_t* __restrict__ rp, const int32_t* __restrict__ heavy, int64_t nh,
+                               int64_t* __restrict__ out) {
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x) {
+        out[2 * h] = rp[heavy[h]];
+        out[2 * h + 1] = rp[heavy[h] + 1];
+    }
+}
+
 void build_heavy(Ctx& c, Level& L) {
     auto mk = c.tmp->save();
     int64_t* d_cnt = c.tmp_alloc<int64_t>(4);
@@ -55,6 +63,46 @@ void build_heavy(Ctx& c, Level& L) {
     for (int b = 0; b < 3; ++b) L.nbucket[b] = c.h_pinned[b];
     L.nheavy = c.h_pinned[3];
     c.tmp->restore(mk);
+    // items: heavy row h covers [rp[v], rp[v+1]) in pieces of at most kHeavyDeg
+    std::vector<int64_t> rb((size_t)std::max<int64_t>(L.nheavy, 1)), re((size_t)std::max<int64_t>(L.nheavy, 1));
+    if (L.nheavy > 0) {
+        // row bounds of the heavy rows
+        int64_t* d_rb = c.tmp_alloc<int64_t>(2 * L.nheavy);
+        k_heavy_bounds<<<grid_for(L.nheavy, 256), 256, 0, c.s>>>(L.g.rp, L.heavy, L.nheavy, d_rb);
+        GP_LAUNCHED(c);
+        std::vector<int64_t> hb((size_t)(2 * L.nheavy));
+        GP_CUDA(cudaMemcpyAsync(hb.data(), d_rb, sizeof(int64_t) * 2 * L.nheavy, cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        c.tmp->restore(mk);
+        for (int64_t h = 0; h < L.nheavy; ++h) { rb[h] = hb[2 * h]; re[h] = hb[2 * h + 1]; }
+    }
+    std::vector<int32_t> irow, rows_items((size_t)std::max<int64_t>(L.nheavy, 1)), rows_first((size_t)std::max<int64_t>(L.nheavy, 1));
+    std::vector<int64_t> ib, ie;
+    for (int64_t h = 0; h < L.nheavy; ++h) {
+        rows_first[h] = (int32_t)irow.size();
+        int32_t cnt = 0;
+        for (int64_t b = rb[h]; b < re[h]; b += kHeavyDeg) {
+            irow.push_back((int32_t)h);
+            ib.push_back(b);
+            ie.push_back(std::min<int64_t>(b + kHeavyDeg, re[h]));
+            ++cnt;
+        }
+        rows_items[h] = cnt;
+    }
+    L.nitems = (int64_t)irow.size();
+    L.item_row = c.keep_alloc<int32_t>(L.nitems);
+    L.item_beg = c.keep_alloc<int64_t>(L.nitems);
+    L.item_end = c.keep_alloc<int64_t>(L.nitems);
+    L.row_items = c.keep_alloc<int32_t>(L.nheavy);
+    L.row_first = c.keep_alloc<int32_t>(L.nheavy);
+    if (L.nitems > 0) {
+        GP_CUDA(cudaMemcpyAsync(L.item_row, irow.data(), sizeof(int32_t) * L.nitems, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(L.item_beg, ib.data(), sizeof(int64_t) * L.nitems, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(L.item_end, ie.data(), sizeof(int64_t) * L.nitems, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(L.row_items, rows_items.data(), sizeof(int32_t) * L.nheavy, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(L.row_first, rows_first.data(), sizeof(int32_t) * L.nheavy, cudaMemcpyHostToDevice, c.s));
+        c.sync();  // host vectors go out of scope
+    }
 }
 
 // ---------------------------------------------------------------- argmax helpers
@@ -95,6 +143,15 @@ struct MatchArgs {
     DGraph g;
     const int32_t* heavy;
     int64_t nheavy;
+    const int32_t* item_row;   // heavy rows split into items (one CTA each)
+    const int64_t* item_beg;
+    const int64_t* item_end;
+    const int32_t* row_items;
+    const int32_t* row_first;
+    int64_t nitems;
+    uint64_t* ikey;            // per-item partial best
+    int32_t* iid;
+    int32_t* hdone;            // per heavy row: items finished (reset by the last)
     const int32_t* list[3];   // rows to process, by degree bucket
     int64_t nlist[3];
     const int32_t* match;
@@ -169,22 +226,46 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
     __shared__ uint64_t sk[32];
     __shared__ int32_t sid[32];
     const int lane = threadIdx.x & 31;
-    if ((int64_t)blockIdx.x < A.nheavy) {
-        const int64_t v = A.heavy[blockIdx.x];
+    if ((int64_t)blockIdx.x < A.nitems) {
+        // one piece of a long row per CTA; the last piece of a row reduces
+        // the partial bests of all its pieces in item order
+        const int32_t h = A.item_row[blockIdx.x];
+        const int64_t v = A.heavy[h];
         if (A.match[v] != -1) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
         const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
         uint64_t bk = 0; int32_t bid = -1;
-        for (int64_t e = A.g.rp[v] + threadIdx.x; e < A.g.rp[v + 1]; e += blockDim.x) {
+        const int64_t end = A.item_end[blockIdx.x];
+        for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < end; e += blockDim.x) {
             const int32_t u = A.g.ci[e];
             if (match_ok<MODE>(A, v, u, vwv))
                 argmax_merge(bk, bid, edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, u)), u);
         }
         block_argmax(bk, bid, sk, sid);
-        if (threadIdx.x < 32) match_emit<MODE>(A, threadIdx.x == 0, v, bid);
+        const int nit = A.row_items[h];
+        __shared__ int s_last;
+        if (threadIdx.x == 0) {
+            s_last = 1;
+            if (nit > 1) {
+                A.ikey[blockIdx.x] = bk;
+                A.iid[blockIdx.x] = bid;
+                __threadfence();
+                s_last = atomicAdd(&A.hdone[h], 1) == nit - 1;
+                if (s_last) {
+                    __threadfence();
+                    bk = 0; bid = -1;
+                    const int32_t f = A.row_first[h];
+                    for (int i = 0; i < nit; ++i)
+                        argmax_merge(bk, bid, __ldcg((const unsigned long long*)&A.ikey[f + i]), __ldcg(&A.iid[f + i]));
+                    A.hdone[h] = 0;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x < 32) match_emit<MODE>(A, threadIdx.x == 0, v, bid);
         return;
     }
-    const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * blockDim.x) >> 5;
+    const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)(gridDim.x - A.nitems) * blockDim.x) >> 5;
     const int64_t U0 = (A.nlist[0] + 3) / 4, U1 = A.nlist[1], U2 = A.nlist[2];
     for (int64_t u = wid; u < U0 + U1 + U2; u += nw) {
         if (u < U0) {
@@ -305,6 +386,12 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     GP_CUDA(cudaMemsetAsync(match, 0xff, sizeof(int32_t) * g.n, c.s));
     MatchArgs A;
     A.g = g; A.heavy = L.heavy; A.nheavy = L.nheavy; A.match = match; A.out = prop; A.salt = salt;
+    A.item_row = L.item_row; A.item_beg = L.item_beg; A.item_end = L.item_end; A.row_items = L.row_items;
+    A.row_first = L.row_first; A.nitems = L.nitems;
+    A.ikey = c.tmp_alloc<uint64_t>(std::max<int64_t>(L.nitems, 1));
+    A.iid = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nitems, 1));
+    A.hdone = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nheavy, 1));
+    memset_async(c, A.hdone, 0, sizeof(int32_t) * std::max<int64_t>(L.nheavy, 1));
     A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0;
     for (int b = 0; b < 3; ++b) { A.list[b] = L.bucket[b]; A.nlist[b] = L.nbucket[b]; }
     int64_t pairs = 0;
@@ -312,7 +399,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     for (int r = 0; r < P.o.match_rounds; ++r) {
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
         if (units == 0 && L.nheavy == 0) break;
-        const int grid = (int)L.nheavy + grid_for(units * 32, 256, c.sm_count * 8);
+        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * 8);
         memset_async(c, d_cnt, 0, 4 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);
@@ -343,7 +430,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
         const int64_t units = (B2.nlist[0] + 3) / 4 + B2.nlist[1] + B2.nlist[2];
-        const int grid = (int)L.nheavy + grid_for(units * 32, 256, c.sm_count * 8);
+        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * 8);
         k_match_scan<1><<<grid, 256, 0, c.s>>>(B2);
         GP_LAUNCHED(c);
         c.bytes += L.scan_bytes() + 4 * g.n;
@@ -419,30 +506,33 @@ __device__ __forceinline__ uint32_t slot_hash(int32_t key, int lg) {
 }
 
 // warp per fine row (CTA per heavy fine row): mapped ids and weights in walk order
-__global__ void __launch_bounds__(256) k_fill_mapped(DGraph g, const int32_t* __restrict__ heavy, int64_t nheavy,
+__global__ void __launch_bounds__(256) k_fill_mapped(DGraph g, const int32_t* __restrict__ heavy,
+                                                     const int32_t* __restrict__ item_row,
+                                                     const int64_t* __restrict__ item_beg,
+                                                     const int64_t* __restrict__ item_end, int64_t nitems,
                                                      const int32_t* __restrict__ cmap, const int32_t* __restrict__ mem,
                                                      const int64_t* __restrict__ off, int32_t* __restrict__ mapped,
                                                      int32_t* __restrict__ mw) {
-    auto fill_row = [&](int64_t x, int start, int stride) {
+    auto fill_range = [&](int64_t x, int64_t from, int64_t to, int start, int stride) {
         const int32_t cc = cmap[x];
         const int32_t a = mem[2 * (int64_t)cc];
         const int64_t base = off[cc] + ((int32_t)x == a ? 0 : g.rp[a + 1] - g.rp[a]);
-        const int64_t beg = g.rp[x], end = g.rp[x + 1];
-        for (int64_t e = beg + start; e < end; e += stride) {
+        const int64_t beg = g.rp[x];
+        for (int64_t e = from + start; e < to; e += stride) {
             mapped[base + (e - beg)] = cmap[g.ci[e]];
             mw[base + (e - beg)] = g.ew ? g.ew[e] : 1;
         }
     };
-    if ((int64_t)blockIdx.x < nheavy) {
-        fill_row(heavy[blockIdx.x], threadIdx.x, blockDim.x);
+    if ((int64_t)blockIdx.x < nitems) {
+        fill_range(heavy[item_row[blockIdx.x]], item_beg[blockIdx.x], item_end[blockIdx.x], threadIdx.x, blockDim.x);
         return;
     }
     const int lane = threadIdx.x & 31;
-    const int64_t wid = ((int64_t)(blockIdx.x - nheavy) * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)(gridDim.x - nheavy) * blockDim.x) >> 5;
+    const int64_t wid = ((int64_t)(blockIdx.x - nitems) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)(gridDim.x - nitems) * blockDim.x) >> 5;
     for (int64_t x = wid; x < g.n; x += nw) {
         if (g.rp[x + 1] - g.rp[x] > kHeavyDeg) continue;
-        fill_row(x, lane, 32);
+        fill_range(x, g.rp[x], g.rp[x + 1], lane, 32);
     }
 }
 
@@ -747,8 +837,9 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     memset_async(c, lcount, 0, 3 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
-        const int grid = (int)fine.nheavy + grid_for(g.n * 32, 256, c.sm_count * 8);
-        k_fill_mapped<<<grid, 256, 0, c.s>>>(g, fine.heavy, fine.nheavy, fine.cmap, mem, off, mapped, mw);
+        const int grid = (int)fine.nitems + grid_for(g.n * 32, 256, c.sm_count * 8);
+        k_fill_mapped<<<grid, 256, 0, c.s>>>(g, fine.heavy, fine.item_row, fine.item_beg, fine.item_end, fine.nitems,
+                                             fine.cmap, mem, off, mapped, mw);
         GP_LAUNCHED(c);
     }
     {

@@ -33,6 +33,13 @@ struct Level {
     int64_t nheavy = 0;
     int32_t* bucket[3] = {nullptr, nullptr, nullptr};
     int64_t nbucket[3] = {0, 0, 0};
+    // heavy rows split into items of at most kHeavyDeg entries, one CTA each
+    int32_t* item_row = nullptr;   // index into heavy[]
+    int64_t* item_beg = nullptr;   // entry range of the item
+    int64_t* item_end = nullptr;
+    int32_t* row_items = nullptr;  // items per heavy row
+    int32_t* row_first = nullptr;  // first item of each heavy row
+    int64_t nitems = 0;
     // bytes of one neighbour scan: row pointers, column ids, weights, gathered per-neighbour int32 state
     int64_t scan_bytes() const { return 8 * (g.n + 1) + 4 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.m; }
 };
@@ -82,6 +89,10 @@ struct RefineBufs {
     int64_t* best_pw = nullptr;   // k
     int64_t* status = nullptr;    // 16
     int32_t* clist[3] = {nullptr, nullptr, nullptr};   // LP candidates by degree bucket
+    // accumulators of heavy rows split over several CTAs (zero between uses)
+    int32_t* hhist = nullptr;     // nheavy_max * k connectivity sums
+    int64_t* hsum = nullptr;      // nheavy_max * 2: cross, total (conn) / gain (afterburner)
+    int32_t* hdone = nullptr;     // nheavy_max: finished items
     uint64_t* ckeys = nullptr;    // rebalance candidate keys
     int32_t* cvals = nullptr;
     uint64_t* ckeys2 = nullptr;

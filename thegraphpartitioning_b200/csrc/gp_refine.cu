@@ -76,14 +76,30 @@ struct ConnArgs {
     const uint8_t* lock;
     const int64_t* pw;
     const int32_t* heavy;
-    int64_t nheavy;
+    const int32_t* item_row;
+    const int64_t* item_beg;
+    const int64_t* item_end;
+    const int32_t* row_items;
+    int64_t nitems;
     const int32_t* bucket[3];
     int64_t nbucket[3];
     int32_t* dest;
     int32_t* gain;
     int64_t* status;
     int32_t* clist[3];
+    int32_t* hhist;
+    int64_t* hsum;
+    int32_t* hdone;
 };
+
+// histogram add with the lanes of a warp that hold the same part combined
+// first (neighbours of dense rows concentrate in few parts); all lanes call
+__device__ __forceinline__ void hist_add(int32_t* hist, int32_t q, int32_t w, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? (uint32_t)q : (0x80000000u | (uint32_t)lane));
+    const int32_t sum = (int32_t)__reduce_add_sync(peers, (uint32_t)w);
+    if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[q], sum);
+}
 
 // warp-aggregated append of the lanes with take set
 __device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, int64_t* count) {
@@ -187,10 +203,9 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
         for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? A.part[u[c]] : -1;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            if (q[c] < 0) continue;
             tot += w[c];
-            if (q[c] != p) cross += w[c];
-            if (active) atomicAdd(&hist[q[c]], w[c]);
+            if (q[c] >= 0 && q[c] != p) cross += w[c];
+            if (active) hist_add(hist, q[c], w[c], q[c] >= 0);
         }
     }
     cross = warp_sum(cross);
@@ -270,13 +285,16 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
     }
     int64_t acc = 0;  // directed cross weight (this thread)
 
-    if ((int64_t)blockIdx.x < A.nheavy) {
-        // ---- one long row per CTA
+    if ((int64_t)blockIdx.x < A.nitems) {
+        // ---- one piece of a long row per CTA; pieces of the same row are
+        // combined in global accumulators and the last CTA decides
         int32_t* hist = hist_all;
-        const int64_t v = A.heavy[blockIdx.x];
+        const int32_t h = A.item_row[blockIdx.x];
+        const int64_t v = A.heavy[h];
+        const int nit = A.row_items[h];
         const int32_t p = A.part[v];
         const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
-        const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
+        const int64_t beg = A.item_beg[blockIdx.x], end = A.item_end[blockIdx.x];
         int64_t cross = 0, tot = 0;
         for (int64_t base = beg; base < end; base += 4 * RT) {
             int32_t uu[4], ww[4], qq[4];
@@ -290,41 +308,71 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
             for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                if (qq[c] < 0) continue;
                 tot += ww[c];
-                if (qq[c] != p) cross += ww[c];
-                if (active) atomicAdd(&hist[qq[c]], ww[c]);
+                if (qq[c] >= 0 && qq[c] != p) cross += ww[c];
+                if (active) hist_add(hist, qq[c], ww[c], qq[c] >= 0);
             }
         }
         cross = warp_sum(cross); tot = warp_sum(tot);
+        acc += (lane == 0) ? cross : 0;  // the cut adds every piece
         __syncthreads();
         if (lane == 0) { s_red[w] = cross; s_k[w] = (uint64_t)tot; }
         __syncthreads();
+        __shared__ int s_last;
         if (threadIdx.x == 0) {
             int64_t c2 = 0, t2 = 0;
             for (int i = 0; i < RW; ++i) { c2 += s_red[i]; t2 += (int64_t)s_k[i]; }
             s_red[0] = c2; s_k[0] = (uint64_t)t2;
+            s_last = 1;
         }
         __syncthreads();
-        cross = s_red[0]; tot = (int64_t)s_k[0];
-        __syncthreads();
-        uint64_t bk = 0; int32_t bq = -1;
-        if (active)
-            for (int q = threadIdx.x; q < k; q += RT)
-                if (q != p && hist[q] > 0 && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
-        warp_argmax_q(bk, bq);
-        if (lane == 0) { s_k[w] = bk; s_q[w] = bq; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int i = 1; i < RW; ++i) argmax_q(bk, bq, s_k[i], s_q[i]);
-            acc += cross;
-            if (conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light))
-                atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
+        if (nit > 1) {
+            if (active)
+                for (int q = threadIdx.x; q < k; q += RT)
+                    if (hist[q]) atomicAdd(&A.hhist[(int64_t)h * k + q], hist[q]);
+            if (threadIdx.x == 0) {
+                atomicAdd((unsigned long long*)&A.hsum[2 * h], (unsigned long long)s_red[0]);
+                atomicAdd((unsigned long long*)&A.hsum[2 * h + 1], (unsigned long long)s_k[0]);
+            }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) s_last = (atomicAdd(&A.hdone[h], 1) == nit - 1) ? 1 : 0;
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                for (int q = threadIdx.x; q < k; q += RT) {
+                    hist[q] = active ? __ldcg(&A.hhist[(int64_t)h * k + q]) : 0;
+                    A.hhist[(int64_t)h * k + q] = 0;
+                }
+                if (threadIdx.x == 0) {
+                    s_red[0] = (int64_t)__ldcg((const unsigned long long*)&A.hsum[2 * h]);
+                    s_k[0] = (uint64_t)__ldcg((const unsigned long long*)&A.hsum[2 * h + 1]);
+                    A.hsum[2 * h] = 0; A.hsum[2 * h + 1] = 0; A.hdone[h] = 0;
+                }
+                __syncthreads();
+            }
+        }
+        if (s_last) {
+            cross = s_red[0]; tot = (int64_t)s_k[0];
+            __syncthreads();
+            uint64_t bk = 0; int32_t bq = -1;
+            if (active)
+                for (int q = threadIdx.x; q < k; q += RT)
+                    if (q != p && hist[q] > 0 && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+            warp_argmax_q(bk, bq);
+            if (lane == 0) { s_k[w] = bk; s_q[w] = bq; }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int i = 1; i < RW; ++i) argmax_q(bk, bq, s_k[i], s_q[i]);
+                const int64_t rdeg = A.g.rp[v + 1] - A.g.rp[v];
+                if (conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light))
+                    atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)rdeg);
+            }
         }
     } else {
         int32_t* hist = hist_all + w * k;
-        const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * RT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * RT) >> 5;
+        const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - A.nitems) * RT) >> 5;
         const int64_t U0 = (A.nbucket[0] + 3) / 4, U1 = A.nbucket[1], U2 = A.nbucket[2];
         for (int64_t u = wid; u < U0 + U1 + U2; u += nw) {
             if (u < U0) {
@@ -378,13 +426,19 @@ struct ApplyArgs {
     const int32_t* dest;
     const int32_t* gain;
     const int32_t* heavy;
-    int64_t nheavy;
+    const int32_t* item_row;
+    const int64_t* item_beg;
+    const int64_t* item_end;
+    const int32_t* row_items;
+    int64_t nitems;
     const int32_t* clist[3];
     const int64_t* status;
     int32_t* part_next;
     uint8_t* lock_next;
     int64_t* pw;
     int64_t* moves_out;
+    int64_t* hsum;
+    int32_t* hdone;
 };
 
 __device__ __forceinline__ void ab_commit(const ApplyArgs& A, int64_t v, int32_t p, int32_t d, int64_t* delta,
@@ -415,33 +469,47 @@ __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* 
 
 __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
     extern __shared__ int64_t delta[];
-    __shared__ int32_t s_red[RW];
+    __shared__ int64_t s_red[RW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int q = threadIdx.x; q < A.k; q += RT) delta[q] = 0;
     __syncthreads();
     int64_t moves = 0;
-    if ((int64_t)blockIdx.x < A.nheavy) {
-        const int64_t v = A.heavy[blockIdx.x];
+    if ((int64_t)blockIdx.x < A.nitems) {
+        const int32_t h = A.item_row[blockIdx.x];
+        const int64_t v = A.heavy[h];
         const int32_t d = A.dest[v];
         if (d >= 0) {
+            const int nit = A.row_items[h];
             const int32_t p = A.part[v], gv = A.gain[v];
             int32_t g2 = 0;
-            for (int64_t e = A.g.rp[v] + threadIdx.x; e < A.g.rp[v + 1]; e += RT)
+            for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < A.item_end[blockIdx.x]; e += RT)
                 g2 += ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
             g2 = warp_sum(g2);
             if (lane == 0) s_red[w] = g2;
             __syncthreads();
             if (threadIdx.x == 0) {
-                int32_t s = 0;
-                for (int i = 0; i < RW; ++i) s += s_red[i];
-                if (s >= 0) ab_commit(A, v, p, d, delta, moves);
+                int64_t sum = 0;
+                for (int i = 0; i < RW; ++i) sum += s_red[i];
+                bool last = true;
+                if (nit > 1) {
+                    atomicAdd((unsigned long long*)&A.hsum[2 * h], (unsigned long long)sum);
+                    __threadfence();
+                    last = atomicAdd(&A.hdone[h], 1) == nit - 1;
+                    if (last) {
+                        __threadfence();
+                        sum = (int64_t)__ldcg((const unsigned long long*)&A.hsum[2 * h]);
+                        A.hsum[2 * h] = 0;
+                        A.hdone[h] = 0;
+                    }
+                }
+                if (last && sum >= 0) ab_commit(A, v, p, d, delta, moves);
             }
         }
     } else {
         const int64_t n0 = A.status[S_NL0], n1 = A.status[S_NL1], n2 = A.status[S_NL2];
         const int64_t U0 = (n0 + 3) / 4;
-        const int64_t wid = ((int64_t)(blockIdx.x - A.nheavy) * RT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)(gridDim.x - A.nheavy) * RT) >> 5;
+        const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * RT + threadIdx.x) >> 5;
+        const int64_t nw = ((int64_t)(gridDim.x - A.nitems) * RT) >> 5;
         for (int64_t u = wid; u < U0 + n1 + n2; u += nw) {
             if (u < U0) {
                 const int64_t i = u * 4 + (lane >> 3);
@@ -707,7 +775,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
     GP_CUDA(cudaFuncSetAttribute(k_conn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conn_smem));
     const int light_blocks = grid_for(n * 32, RT, c.sm_count * 8);
-    const int grid = (int)L.nheavy + light_blocks;
+    const int grid = (int)L.nitems + light_blocks;
     int64_t best_cut = 0, best_mp = 0;
     int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
     int64_t prev_moves = -1;
@@ -718,7 +786,9 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_a, c.s));
         ConnArgs CA;
         CA.g = g; CA.k = k; CA.Lmax = Lmax; CA.den = P.o.lp_filter_den; CA.force_eval = final_eval ? 1 : 0;
-        CA.part = B.part; CA.lock = B.lock; CA.pw = B.pw; CA.heavy = L.heavy; CA.nheavy = L.nheavy;
+        CA.part = B.part; CA.lock = B.lock; CA.pw = B.pw; CA.heavy = L.heavy;
+        CA.item_row = L.item_row; CA.item_beg = L.item_beg; CA.item_end = L.item_end; CA.row_items = L.row_items;
+        CA.nitems = L.nitems; CA.hhist = B.hhist; CA.hsum = B.hsum; CA.hdone = B.hdone;
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = L.bucket[b]; CA.nbucket[b] = L.nbucket[b]; CA.clist[b] = B.clist[b]; }
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
         k_conn<<<grid, RT, conn_smem, c.s>>>(CA);
@@ -779,7 +849,8 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             GP_LAUNCHED(c);
             ApplyArgs AA;
             AA.g = g; AA.k = k; AA.part = B.part; AA.dest = B.dest; AA.gain = B.gain; AA.heavy = L.heavy;
-            AA.nheavy = L.nheavy;
+            AA.item_row = L.item_row; AA.item_beg = L.item_beg; AA.item_end = L.item_end; AA.row_items = L.row_items;
+            AA.nitems = L.nitems; AA.hsum = B.hsum; AA.hdone = B.hdone;
             for (int b = 0; b < 3; ++b) AA.clist[b] = B.clist[b];
             AA.status = B.status; AA.part_next = B.part_next; AA.lock_next = B.lock_next; AA.pw = B.pw;
             AA.moves_out = moves_d;
