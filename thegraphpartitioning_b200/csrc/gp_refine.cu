@@ -92,13 +92,8 @@ struct ConnArgs {
     int32_t* hdone;
 };
 
-// histogram add with the lanes of a warp that hold the same part combined
-// first (neighbours of dense rows concentrate in few parts); all lanes call
 __device__ __forceinline__ void hist_add(int32_t* hist, int32_t q, int32_t w, bool valid) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? (uint32_t)q : (0x80000000u | (uint32_t)lane));
-    const int32_t sum = (int32_t)__reduce_add_sync(peers, (uint32_t)w);
-    if (valid && lane == __ffs(peers) - 1) atomicAdd(&hist[q], sum);
+    if (valid) atomicAdd(&hist[q], w);
 }
 
 // warp-aggregated append of the lanes with take set
