@@ -48,6 +48,23 @@ __global__ void k_heavy_bounds(const int64_t* __restrict__ rp, const int32_t* __
     }
 }
 
+// cost of light unit u (order: bucket 2, bucket 1, groups of 4 of bucket 0)
+__global__ void k_unit_cost(const int64_t* __restrict__ rp, const int32_t* __restrict__ b0, int64_t n0,
+                            const int32_t* __restrict__ b1, int64_t n1, const int32_t* __restrict__ b2, int64_t n2,
+                            int64_t* __restrict__ cost) {
+    const int64_t U0 = (n0 + 3) / 4, U = n2 + n1 + U0;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < U; u += (int64_t)gridDim.x * blockDim.x) {
+        int64_t cst = 32;
+        if (u < n2) cst += rp[b2[u] + 1] - rp[b2[u]];
+        else if (u < n2 + n1) cst += rp[b1[u - n2] + 1] - rp[b1[u - n2]];
+        else {
+            const int64_t g = u - n2 - n1;
+            for (int i = 0; i < 4 && 4 * g + i < n0; ++i) cst += rp[b0[4 * g + i] + 1] - rp[b0[4 * g + i]];
+        }
+        cost[u] = cst;
+    }
+}
+
 void build_heavy(Ctx& c, Level& L) {
     auto mk = c.tmp->save();
     int64_t* d_cnt = c.tmp_alloc<int64_t>(4);
@@ -81,15 +98,25 @@ void build_heavy(Ctx& c, Level& L) {
     for (int64_t h = 0; h < L.nheavy; ++h) {
         rows_first[h] = (int32_t)irow.size();
         int32_t cnt = 0;
-        for (int64_t b = rb[h]; b < re[h]; b += kHeavyDeg) {
+        for (int64_t b = rb[h]; b < re[h]; b += kItemLen) {
             irow.push_back((int32_t)h);
             ib.push_back(b);
-            ie.push_back(std::min<int64_t>(b + kHeavyDeg, re[h]));
+            ie.push_back(std::min<int64_t>(b + kItemLen, re[h]));
             ++cnt;
         }
         rows_items[h] = cnt;
     }
     L.nitems = (int64_t)irow.size();
+    {
+        L.nunits = L.nbucket[2] + L.nbucket[1] + (L.nbucket[0] + 3) / 4;
+        int64_t* cost = c.tmp_alloc<int64_t>(L.nunits + 1);
+        L.unit_cost = c.keep_alloc<int64_t>(L.nunits + 1);
+        k_unit_cost<<<grid_for(L.nunits, 256), 256, 0, c.s>>>(L.g.rp, L.bucket[0], L.nbucket[0], L.bucket[1],
+                                                              L.nbucket[1], L.bucket[2], L.nbucket[2], cost);
+        GP_LAUNCHED(c);
+        scan_excl_i64(c, cost, L.unit_cost, L.nunits, L.unit_cost + L.nunits);
+        c.tmp->restore(mk);
+    }
     L.item_row = c.keep_alloc<int32_t>(L.nitems);
     L.item_beg = c.keep_alloc<int64_t>(L.nitems);
     L.item_end = c.keep_alloc<int64_t>(L.nitems);

@@ -136,7 +136,8 @@ inline int grid_for(int64_t items, int per_block, int cap = 148 * 16) {
     if (g > cap) g = cap;
     return (int)g;
 }
-constexpr int kHeavyDeg = 16384;  // rows longer than this take a whole CTA
+constexpr int kHeavyDeg = 2048;   // rows longer than this take whole CTAs
+constexpr int kItemLen = 16384;   // entries of one CTA item of a long row
 
 // ---------------------------------------------------------------- primitives (gp_prims.cu)
 // exclusive scan; out may alias in; returns total on the host if total_out != nullptr

@@ -40,6 +40,11 @@ struct Level {
     int32_t* row_items = nullptr;  // items per heavy row
     int32_t* row_first = nullptr;  // first item of each heavy row
     int64_t nitems = 0;
+    // light work units in the order bucket 2 rows, bucket 1 rows, groups of 4
+    // bucket 0 rows, with the prefix sum of their costs (entries + 32): warps
+    // take contiguous unit ranges of equal cost
+    int64_t* unit_cost = nullptr;  // nunits + 1 prefix
+    int64_t nunits = 0;
     // bytes of one neighbour scan: row pointers, column ids, weights, gathered per-neighbour int32 state
     int64_t scan_bytes() const { return 8 * (g.n + 1) + 4 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.m; }
 };

@@ -83,6 +83,8 @@ struct ConnArgs {
     int64_t nitems;
     const int32_t* bucket[3];
     int64_t nbucket[3];
+    const int64_t* unit_cost;   // prefix of unit costs (nunits + 1)
+    int64_t nunits;
     int32_t* dest;
     int32_t* gain;
     int64_t* status;
@@ -368,15 +370,26 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
         int32_t* hist = hist_all + w * k;
         const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * RT + threadIdx.x) >> 5;
         const int64_t nw = ((int64_t)(gridDim.x - A.nitems) * RT) >> 5;
-        const int64_t U0 = (A.nbucket[0] + 3) / 4, U1 = A.nbucket[1], U2 = A.nbucket[2];
-        for (int64_t u = wid; u < U0 + U1 + U2; u += nw) {
-            if (u < U0) {
-                const int64_t i = u * 4 + (lane >> 3);
-                conn_tile<kTile8>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
-            } else if (u < U0 + U1) {
-                conn_tile<kTile32>(A, A.bucket[1][u - U0], mode, over, light, 1, acc);
+        const int64_t U2 = A.nbucket[2], U1 = A.nbucket[1];
+        // contiguous units of equal total cost: [first unit with prefix >= wid*T/nw, ...)
+        const int64_t T = A.unit_cost[A.nunits];
+        auto first_unit = [&](int64_t target) {
+            int64_t lo = 0, hi = A.nunits;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (A.unit_cost[mid] < target) lo = mid + 1; else hi = mid;
+            }
+            return lo;
+        };
+        const int64_t u0 = first_unit((T * wid) / nw), u1 = first_unit((T * (wid + 1)) / nw);
+        for (int64_t u = u0; u < u1; ++u) {
+            if (u < U2) {
+                conn_warp(A, A.bucket[2][u], mode, over, light, hist, acc);
+            } else if (u < U2 + U1) {
+                conn_tile<kTile32>(A, A.bucket[1][u - U2], mode, over, light, 1, acc);
             } else {
-                conn_warp(A, A.bucket[2][u - U0 - U1], mode, over, light, hist, acc);
+                const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
+                conn_tile<kTile8>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
             }
         }
     }
@@ -785,6 +798,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         CA.item_row = L.item_row; CA.item_beg = L.item_beg; CA.item_end = L.item_end; CA.row_items = L.row_items;
         CA.nitems = L.nitems; CA.hhist = B.hhist; CA.hsum = B.hsum; CA.hdone = B.hdone;
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = L.bucket[b]; CA.nbucket[b] = L.nbucket[b]; CA.clist[b] = B.clist[b]; }
+        CA.unit_cost = L.unit_cost; CA.nunits = L.nunits;
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
         k_conn<<<grid, RT, conn_smem, c.s>>>(CA);
         GP_LAUNCHED(c);
