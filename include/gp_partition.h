@@ -165,6 +165,27 @@ int gp_edge_cut_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_coli
                        const int32_t* d_part, int32_t k, void* stream,
                        int64_t* cut_out, int64_t* part_weights_out);
 
+/* Largest k accepted by gp_edge_cut_device_noalloc. */
+#define GP_NOALLOC_MAX_K 1024
+
+/* No counterpart in the reference (which has no library API).
+ * Same result as gp_edge_cut_device, for callers that must not allocate:
+ * code running while a CUDA graph is captured on its stream, code inside an
+ * allocator or memory-pool callback, loops that forbid allocation after
+ * start-up, processes whose device memory another framework has reserved.
+ * gp_edge_cut_device may grow a cached workspace with cudaMalloc on first use;
+ * this variant calls no cudaMalloc, cudaFree or other allocating routine.  Its
+ * scratch is a fixed array in device memory (about 8 KB, held by every device
+ * that loads the library until the process exits), so k must not exceed
+ * GP_NOALLOC_MAX_K (GP_EINVAL otherwise).  All calls on a device share that
+ * array: calls that overlap on the GPU race and must be serialized by the
+ * caller.  The first call on each device looks up the array's address; make
+ * it before any stream capture.  Synchronizes `stream`. */
+int gp_edge_cut_device_noalloc(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                               const int32_t* d_ewgt, const int32_t* d_vwgt,
+                               const int32_t* d_part, int32_t k, void* stream,
+                               int64_t* cut_out, int64_t* part_weights_out);
+
 /* Release cached device workspaces of the current device. */
 int gp_release_workspace(void);
 
