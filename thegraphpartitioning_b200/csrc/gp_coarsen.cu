@@ -226,10 +226,10 @@ __device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
     if (valid) {
         const int64_t e = A.g.rp[v] + tl;
         if (e < A.g.rp[v + 1]) {
-            const int32_t u = A.g.ci[e];
+            const int32_t u = __ldcs(&A.g.ci[e]);
             const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
             if (match_ok<MODE>(A, v, u, vwv)) {
-                bk = edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, u));
+                bk = edge_key(A.g.ew ? __ldcs(&A.g.ew[e]) : 1, edge_hash(A.salt, (int32_t)v, u));
                 bid = u;
             }
         }
@@ -263,9 +263,9 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
         uint64_t bk = 0; int32_t bid = -1;
         const int64_t end = A.item_end[blockIdx.x];
         for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < end; e += blockDim.x) {
-            const int32_t u = A.g.ci[e];
+            const int32_t u = __ldcs(&A.g.ci[e]);
             if (match_ok<MODE>(A, v, u, vwv))
-                argmax_merge(bk, bid, edge_key(A.g.ew ? A.g.ew[e] : 1, edge_hash(A.salt, (int32_t)v, u)), u);
+                argmax_merge(bk, bid, edge_key(A.g.ew ? __ldcs(&A.g.ew[e]) : 1, edge_hash(A.salt, (int32_t)v, u)), u);
         }
         block_argmax(bk, bid, sk, sid);
         const int nit = A.row_items[h];
@@ -312,8 +312,8 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const int64_t e = base + c * 32 + lane;
-                        uu[c] = e < end ? A.g.ci[e] : -1;
-                        ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+                        uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
+                        ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -546,8 +546,8 @@ __global__ void __launch_bounds__(256) k_fill_mapped(DGraph g, const int32_t* __
         const int64_t base = off[cc] + ((int32_t)x == a ? 0 : g.rp[a + 1] - g.rp[a]);
         const int64_t beg = g.rp[x];
         for (int64_t e = from + start; e < to; e += stride) {
-            mapped[base + (e - beg)] = cmap[g.ci[e]];
-            mw[base + (e - beg)] = g.ew ? g.ew[e] : 1;
+            mapped[base + (e - beg)] = cmap[__ldcs(&g.ci[e])];
+            mw[base + (e - beg)] = g.ew ? __ldcs(&g.ew[e]) : 1;
         }
     };
     if ((int64_t)blockIdx.x < nitems) {

@@ -147,7 +147,7 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     const int64_t e = beg + tl;
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
-    if (has) { q = A.part[A.g.ci[e]]; w = A.g.ew ? A.g.ew[e] : 1; }
+    if (has) { q = A.part[__ldcs(&A.g.ci[e])]; w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
     int32_t cross = (has && q != p) ? w : 0, tot = w;
 #pragma unroll
     for (int o = TILE / 2; o > 0; o >>= 1) {
@@ -193,8 +193,8 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int64_t e = base + c * 32 + lane;
-            u[c] = e < end ? A.g.ci[e] : -1;
-            w[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+            u[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
+            w[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? A.part[u[c]] : -1;
@@ -221,12 +221,12 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
             for (int q = lane; q < A.k; q += 32) hist[q] = 0;
         } else {
             for (int64_t e = beg + lane; e < end; e += 32) {
-                const int32_t q = A.part[A.g.ci[e]];
+                const int32_t q = A.part[__ldcs(&A.g.ci[e])];
                 if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
             }
             warp_argmax_q(bk, bq);
             __syncwarp();
-            for (int64_t e = beg + lane; e < end; e += 32) hist[A.part[A.g.ci[e]]] = 0;
+            for (int64_t e = beg + lane; e < end; e += 32) hist[A.part[__ldcs(&A.g.ci[e])]] = 0;
         }
         __syncwarp();
     }
@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int64_t e = base + c * RT + threadIdx.x;
-                uu[c] = e < end ? A.g.ci[e] : -1;
-                ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+                uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
+                ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
             }
 #pragma unroll
             for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
@@ -416,14 +416,14 @@ __global__ void k_copy_state(int64_t n, const int32_t* __restrict__ part, int32_
 __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v, int32_t p, int32_t d, int32_t gv,
                                            const int32_t* __restrict__ part, const int32_t* __restrict__ dest,
                                            const int32_t* __restrict__ gain) {
-    const int32_t u = g.ci[e];
+    const int32_t u = __ldcs(&g.ci[e]);
     int32_t pu = part[u];
     const int32_t du = dest[u];
     if (du >= 0) {
         const int32_t gu = gain[u];
         if (gu > gv || (gu == gv && u < (int32_t)v)) pu = du;
     }
-    const int32_t wt = g.ew ? g.ew[e] : 1;
+    const int32_t wt = g.ew ? __ldcs(&g.ew[e]) : 1;
     return pu == d ? wt : (pu == p ? -wt : 0);
 }
 
@@ -534,8 +534,8 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const int64_t e = base + c * 32 + lane;
-                        uu[c] = e < end ? A.g.ci[e] : -1;
-                        ww[c] = e < end ? (A.g.ew ? A.g.ew[e] : 1) : 0;
+                        uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
+                        ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(RT) k_cut(DGraph g, const int32_t* __restrict_
     for (int64_t v = wid; v < g.n; v += nw) {
         const int32_t p = part[v];
         for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32)
-            if (part[g.ci[e]] != p) acc += g.ew ? g.ew[e] : 1;
+            if (part[__ldcs(&g.ci[e])] != p) acc += g.ew ? __ldcs(&g.ew[e]) : 1;
     }
     acc = warp_sum(acc);
     if (lane == 0) s_red[w] = acc;
