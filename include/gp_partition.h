@@ -165,6 +165,23 @@ int gp_edge_cut_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_coli
                        const int32_t* d_part, int32_t k, void* stream,
                        int64_t* cut_out, int64_t* part_weights_out);
 
+/* Batched mode (no counterpart in the reference): partition ngraphs
+ * independent graphs held in device memory in one call.  Graph i is given by
+ * ns[i] vertices, ms[i] directed entries and device pointers rowptrs[i],
+ * colidxs[i], vwgts[i] (array or entries may be NULL), ewgts[i]; its result,
+ * ns[i] part ids in [0, ks[i]), goes to parts_out[i].  Every graph's result is
+ * exactly what gp_partition_device returns for it with the same k, imbalance,
+ * seed and options.  `workers` concurrent streams (0: 16) take the graphs
+ * largest first (by n + m); work starts after prior work on `stream` and
+ * `stream` is ordered after all of it.  stats: ngraphs records or NULL.
+ * Synchronous. */
+int gp_partition_batch_device(int32_t ngraphs, const int64_t* ns, const int64_t* ms,
+                              const int64_t* const* d_rowptrs, const int32_t* const* d_colidxs,
+                              const int32_t* const* d_vwgts, const int32_t* const* d_ewgts,
+                              const int32_t* ks, const float* imbalances, const uint64_t* seeds,
+                              int32_t* const* d_parts_out, void* stream, int32_t workers,
+                              const gp_options* opt, gp_stats* stats);
+
 /* Largest k accepted by gp_edge_cut_device_noalloc. */
 #define GP_NOALLOC_MAX_K 1024
 

@@ -63,6 +63,11 @@ def lib():
     L.gp_edge_cut_device.restype = C.c_int
     L.gp_edge_cut_device.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_int32, C.c_void_p, P64, P64]
+    PP64, PP32 = C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)
+    L.gp_partition_batch_device.restype = C.c_int
+    L.gp_partition_batch_device.argtypes = [C.c_int32, P64, P64, PP64, PP32, PP32, PP32, P32, C.POINTER(C.c_float),
+                                            C.POINTER(C.c_uint64), PP32, C.c_void_p, C.c_int32,
+                                            C.POINTER(GpOptions), C.POINTER(GpStats)]
     L.gp_default_options.restype = C.c_int
     L.gp_default_options.argtypes = [C.POINTER(GpOptions)]
     L.gp_release_workspace.restype = C.c_int
@@ -147,6 +152,59 @@ def edge_cut(rowptr, colidx, part, k: int, ewgt=None, vwgt=None, stream=None):
                               C.c_void_p(stream), C.byref(cut), i64p(pw))
     _check(rc)
     return int(cut.value), pw
+
+
+def partition_batch(graphs, ks, imbalances=0.03, seeds=0, options=None, workers=0, stream=None, outs=None):
+    """Partition many independent graphs (torch CUDA tensors) in one call.
+
+    graphs: list of (rowptr int64, colidx int32[, vwgt, ewgt]) on one device.
+    ks / imbalances / seeds: per graph, or one value for all.  Returns
+    (parts: list of int32 CUDA tensors, stats: list of dicts).  Each result is
+    exactly what partition() returns for that graph alone."""
+    import torch
+    L = lib()
+    G = len(graphs)
+    if G == 0:
+        return [], []
+    per = lambda x, t: list(x) if isinstance(x, (list, tuple)) else [x] * G
+    ks, imbs, sds = per(ks, int), per(imbalances, float), per(seeds, int)
+    dev = graphs[0][0].device
+    ns = np.array([g[0].numel() - 1 for g in graphs], dtype=np.int64)
+    ms = np.array([g[1].numel() for g in graphs], dtype=np.int64)
+    parts = outs if outs is not None else [torch.empty(int(n), dtype=torch.int32, device=dev) for n in ns]
+    vp = lambda ts: (C.c_void_p * G)(*[t.data_ptr() if t is not None else None for t in ts])
+    rps = vp([g[0] for g in graphs])
+    cis = vp([g[1] for g in graphs])
+    vws = vp([g[2] if len(g) > 2 else None for g in graphs])
+    ews = vp([g[3] if len(g) > 3 else None for g in graphs])
+    pos = vp(parts)
+    karr = np.ascontiguousarray(ks, dtype=np.int32)
+    iarr = np.ascontiguousarray(imbs, dtype=np.float32)
+    sarr = np.ascontiguousarray([s & 0xFFFFFFFFFFFFFFFF for s in sds], dtype=np.uint64)
+    st = (GpStats * G)()
+    opt = _opts(options)
+    if stream is None:
+        stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = L.gp_partition_batch_device(G, i64p(ns), i64p(ms), rps, cis, vws, ews, i32p(karr),
+                                     iarr.ctypes.data_as(C.POINTER(C.c_float)),
+                                     sarr.ctypes.data_as(C.POINTER(C.c_uint64)), pos, C.c_void_p(stream),
+                                     int(workers), C.byref(opt), st)
+    _check(rc)
+    return parts, [st[i].as_dict() for i in range(G)]
+
+
+def shard_graphs(costs, world: int):
+    """Deterministic longest-processing-time assignment of graphs to ranks:
+    graphs in decreasing cost (ties: lower index) go to the least loaded rank
+    (ties: lower rank).  Returns one index list per rank, each in that order."""
+    order = sorted(range(len(costs)), key=lambda i: (-int(costs[i]), i))
+    load = [0] * world
+    shards = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda j: (load[j], j))
+        shards[r].append(i)
+        load[r] += int(costs[i])
+    return shards
 
 
 def default_options() -> GpOptions:

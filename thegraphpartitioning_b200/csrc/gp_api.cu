@@ -206,8 +206,8 @@ struct Timer {
     double ms(int a, int b) { float t = 0; cudaEventElapsedTime(&t, e[a], e[b]); return t; }
 };
 
-static void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
-                       int32_t* d_out, gp_stats* st, const Tracer& tr) {
+void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
+                int32_t* d_out, gp_stats* st, const Tracer& tr) {
     Params P;
     resolve_options(opt, k, &P.o);
     P.k = k; P.seed = seed; P.imbalance = imbalance;
@@ -379,7 +379,7 @@ struct CallGuard {
     }
 };
 
-static int check_args(int64_t n, int32_t k, float imbalance) {
+int check_args(int64_t n, int32_t k, float imbalance) {
     if (n < 0) throw GpError(GP_EINVAL, "n must be >= 0");
     if (k < 1 || k > GP_MAX_K) throw GpError(GP_EINVAL, "k must be in [1, " + std::to_string(GP_MAX_K) + "]");
     if (!(imbalance >= 0.0f) || !std::isfinite(imbalance)) throw GpError(GP_EINVAL, "imbalance must be finite and >= 0");
@@ -541,6 +541,7 @@ int gp_release_workspace(void) {
         std::lock_guard<std::mutex> lk(S->mu);
         S->keep.release();
         S->tmp.release();
+        release_batch_workers(dev);
     });
 }
 

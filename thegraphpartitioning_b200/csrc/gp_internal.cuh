@@ -109,6 +109,15 @@ struct RefineBufs {
 enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NL0 = 3, S_NL1 = 4, S_LIGHT = 5, S_NL2 = 6, S_CDEG = 7,
                   S_NRESET = 8, S_STEP_MOVES = 8, S_NSLOTS = 16 };
 
+// gp_api.cu
+void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
+                int32_t* d_out, gp_stats* st, const Tracer& tr);
+int check_args(int64_t n, int32_t k, float imbalance);
+extern thread_local std::string t_err;
+
+// gp_batch.cu
+void release_batch_workers(int dev);
+
 // gp_coarsen.cu
 void build_heavy(Ctx& c, Level& L);
 int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out);

@@ -82,8 +82,6 @@ static unsigned long long* noalloc_scratch(int dev) {
     return ptr[dev];
 }
 
-extern thread_local std::string t_err;
-
 }  // namespace gp
 
 using namespace gp;

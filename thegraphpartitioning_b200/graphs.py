@@ -293,3 +293,27 @@ def random_geometric(n: int, mean_degree: float = 8.0, seed: int = 0, device="cp
 
 def undirected_edges(rowptr) -> int:
     return int(rowptr[-1]) // 2
+
+
+def batch_specs(count: int = 4096, seed: int = 0, nmin: int = 1000, nmax: int = 200_000,
+                ks=(2, 4, 8, 16, 32)):
+    """Specs of the batched workload: graph i has n log-uniform in [nmin, nmax],
+    is a random geometric graph (mean degree 8) when i is even and an
+    Erdos-Renyi graph (mean degree 10) when odd, k drawn from ks, and its own
+    seed; all from hashes of (seed, i).  Returns a list of dicts."""
+    specs = []
+    for i in range(count):
+        h = _mix64_int(stream_salt(seed, 1000 + i) & ((1 << 64) - 1))
+        u = (h >> 11) / float(1 << 53)
+        n = int(round(math.exp(math.log(nmin) + u * (math.log(nmax) - math.log(nmin)))))
+        k = ks[(h >> 3) % len(ks)]
+        specs.append({"i": i, "n": n, "k": k, "kind": "rgg" if i % 2 == 0 else "er",
+                      "seed": _mix64_int(h ^ 0x5851F42D4C957F2D)})
+    return specs
+
+
+def batch_graph(spec, device="cpu"):
+    """(rowptr, colidx) of one batch spec."""
+    if spec["kind"] == "rgg":
+        return random_geometric(spec["n"], 8.0, seed=spec["seed"], device=device)
+    return erdos_renyi(spec["n"], 10.0, seed=spec["seed"], device=device)
