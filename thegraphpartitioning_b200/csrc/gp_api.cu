@@ -35,7 +35,19 @@ static DevState* dev_state(int dev) {
     return states[dev].get();
 }
 
+void ensure_kernel_caps(int dev) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    if (dev < 0 || dev >= 64) throw GpError(GP_EINVAL, "device index out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    coarsen_smem_caps();
+    initpart_smem_caps();
+    done[dev] = true;
+}
+
 static void ensure_init(DevState& S, int dev) {
+    ensure_kernel_caps(dev);
     if (S.init) return;
     GP_CUDA(cudaDeviceGetAttribute(&S.sm_count, cudaDevAttrMultiProcessorCount, dev));
     GP_CUDA(cudaMallocHost(&S.pinned, 64 * sizeof(int64_t)));

@@ -79,6 +79,7 @@ extern "C" int gp_partition_batch_device(int32_t ngraphs, const int64_t* ns, con
         GP_CUDA(cudaGetDevice(&dev));
         int sms = 148;
         GP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        ensure_kernel_caps(dev);
         BatchPool* P = batch_pool(dev);
         std::lock_guard<std::mutex> lk(P->mu);
         while ((int32_t)P->workers.size() < workers) {

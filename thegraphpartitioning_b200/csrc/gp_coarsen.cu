@@ -874,8 +874,6 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
         auto kA = k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>;
         auto kB = k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>;
-        GP_CUDA(cudaFuncSetAttribute(kA, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA));
-        GP_CUDA(cudaFuncSetAttribute(kB, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
         kA<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, smA, c.s>>>(nc, 0, off, cdeg, mapped, mw, tci, tew, rowcnt);
         GP_LAUNCHED(c);
         kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * 6), TB_WARPS * 32, smB, c.s>>>(nc, TA_ROW + 1, off, cdeg,
@@ -889,7 +887,6 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
     if (nC > 0) {
         const size_t smem = sizeof(int32_t) * (3 * TC_SLOTS + 2 * ((TC_ROW + 31) / 32));
-        GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * 2), TC_T, smem, c.s>>>(
             listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
@@ -925,6 +922,19 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     coarse.g.ew = cew;
     coarse.g.vw = cvw;
     c.tmp->restore(mk);
+}
+
+// shared-memory caps of the contraction kernels above 48 KB; set once per
+// device (the cap is per kernel and shared by every thread of the process)
+void coarsen_smem_caps() {
+    constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
+    constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
+    const size_t smC = sizeof(int32_t) * (3 * TC_SLOTS + 2 * ((TC_ROW + 31) / 32));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smA));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
 }
 
 }  // namespace gp

@@ -246,7 +246,6 @@ int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out
     int64_t* tmaxpw = c.tmp_alloc<int64_t>(T);
     int64_t* best = c.tmp_alloc<int64_t>(1);
     const size_t smem = (size_t)P.k * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
-    GP_CUDA(cudaFuncSetAttribute(k_initpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int key_iters = bits_for64(n * (n + 1)) + 1;
     k_initpart<<<T, IP_T, smem, c.s>>>(L.g, P.k, P.seed, labels, dists, tcut, tmaxpw, key_iters);
     GP_LAUNCHED(c);
@@ -257,6 +256,13 @@ int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out
     c.bytes += (int64_t)T * (L.scan_bytes() * 4 + 8 * n);
     c.tmp->restore(mk);
     return bt;
+}
+
+// the per-label arrays of k_initpart for the largest k; set once per device
+// (the cap is per kernel, shared by every thread of the process)
+void initpart_smem_caps() {
+    const size_t smem = (size_t)GP_MAX_K * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
+    GP_CUDA(cudaFuncSetAttribute(k_initpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 }
 
 }  // namespace gp

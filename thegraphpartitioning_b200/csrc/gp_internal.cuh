@@ -115,8 +115,13 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
 int check_args(int64_t n, int32_t k, float imbalance);
 extern thread_local std::string t_err;
 
+void ensure_kernel_caps(int dev);   // once per device, before any launch
+
 // gp_batch.cu
 void release_batch_workers(int dev);
+// per-file shared-memory caps (gp_coarsen.cu, gp_initpart.cu)
+void coarsen_smem_caps();
+void initpart_smem_caps();
 
 // gp_coarsen.cu
 void build_heavy(Ctx& c, Level& L);
