@@ -103,7 +103,8 @@ enum gp_trace_kind {
     GP_TR_INITPART = 3,    /* a0 = part[n] of the kept trial; iter = trial id        */
     GP_TR_REFINE_ITER = 4, /* a0 = dest[n] (-1: no proposal), a1 = gain[n],
                               a2 = part[n] after the iteration; cut/maxpw before it   */
-    GP_TR_LEVEL_DONE = 5   /* a0 = part[n] after refinement of this level             */
+    GP_TR_LEVEL_DONE = 5,  /* a0 = part[n] after refinement of this level             */
+    GP_TR_PRIO = 6         /* learned mode: a0 = matching priority per entry (m)       */
 };
 
 typedef struct gp_trace_event {
@@ -181,6 +182,57 @@ int gp_partition_batch_device(int32_t ngraphs, const int64_t* ns, const int64_t*
                               const int32_t* ks, const float* imbalances, const uint64_t* seeds,
                               int32_t* const* d_parts_out, void* stream, int32_t workers,
                               const gp_options* opt, gp_stats* stats);
+
+/* ---- learned matching priorities (no counterpart in the reference; its run
+ * log names a GNNcoarsening.cu that is not in the repository) ------------- */
+typedef struct gp_gnn gp_gnn;   /* a small message-passing edge scorer, device resident */
+
+int gp_gnn_num_params(void);
+int gp_gnn_create(gp_gnn** out);                 /* zero weights */
+int gp_gnn_destroy(gp_gnn* model);
+int gp_gnn_set_params(gp_gnn* model, const float* params, int32_t nparams);   /* host FP32 */
+int gp_gnn_get_params(const gp_gnn* model, float* params, int32_t nparams);
+/* resolution of the matching priority: rint(logit * 2^bits) + 2^30, bits in
+ * [0, 16] (default 16); coarser steps leave near-equal scores to the seeded
+ * hash tie-break */
+int gp_gnn_set_prio_bits(gp_gnn* model, int32_t bits);
+int gp_gnn_get_prio_bits(const gp_gnn* model);
+/* per-entry priorities (int32, may be NULL) and logits (float, may be NULL) of one graph */
+int gp_gnn_forward_device(gp_gnn* model, int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                          const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t level, void* stream,
+                          int32_t* d_prio_out, float* d_logit_out);
+/* mean binary cross-entropy of the edge logits against d_label (1: both ends in one
+ * part) and its gradient (host, gp_gnn_num_params() floats) */
+int gp_gnn_grad_device(gp_gnn* model, int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                       const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t level, const uint8_t* d_label,
+                       void* stream, float* loss_out, float* grad_out);
+/* one Adam step on the gradients summed over ngraphs labelled graphs */
+int gp_gnn_train_step_device(gp_gnn* model, int32_t ngraphs, const int64_t* ns, const int64_t* const* d_rowptrs,
+                             const int32_t* const* d_colidxs, const int32_t* const* d_vwgts,
+                             const int32_t* const* d_ewgts, const int32_t* levels,
+                             const uint8_t* const* d_labels, float lr, void* stream, float* loss_out);
+typedef struct gp_learned_report {
+    int64_t cut_learned;              /* exact cut of the learned V-cycle             */
+    int64_t cut_plain;                /* exact cut of the plain V-cycle (judge != 0)   */
+    int64_t max_part_weight_learned;
+    int64_t max_part_weight_plain;
+    double  ms_learned;               /* device time of each V-cycle                   */
+    double  ms_plain;
+    double  ms_gnn;                   /* part of ms_learned spent in the scorer        */
+    int32_t kept_learned;             /* 1: d_part_out holds the learned partition     */
+    int32_t reserved;
+} gp_learned_report;
+
+/* V-cycle whose matching priority at every level is the model's score instead
+ * of the edge weight; all other rules unchanged.  judge != 0 also runs the
+ * plain V-cycle and keeps the learned partition only when it is within the
+ * balance bound (or the plain one is not) and its exact cut <= the plain cut;
+ * stats describe the partition returned.  The trace covers the learned run. */
+int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
+                                const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t k, float imbalance,
+                                uint64_t seed, int32_t* d_part_out, void* stream, const gp_options* opt,
+                                gp_stats* stats, const gp_gnn* model, int32_t judge, gp_learned_report* report,
+                                gp_trace_fn trace, void* trace_user);
 
 /* Largest k accepted by gp_edge_cut_device_noalloc. */
 #define GP_NOALLOC_MAX_K 1024

@@ -17,7 +17,7 @@ import subprocess
 import numpy as np
 
 from thegraphpartitioning_b200._abi import (
-    GpOptions, GpStats, TraceCollector, make_options, i32p, i64p,
+    GpOptions, GpStats, TraceCollector, make_options, i32p, i64p, PRIO_FN,
 )
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -45,6 +45,8 @@ def _load():
             C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
             C.POINTER(C.c_int32), C.c_int32, C.c_float, C.c_uint64, C.POINTER(C.c_int32),
             C.POINTER(GpOptions), C.POINTER(GpStats), C.c_void_p, C.c_void_p]
+        lib.gpo_partition_prio.restype = C.c_int
+        lib.gpo_partition_prio.argtypes = lib.gpo_partition.argtypes + [C.c_void_p, C.c_void_p]
         lib.gpo_edge_cut.restype = C.c_int
         lib.gpo_edge_cut.argtypes = [
             C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -74,8 +76,12 @@ def _as(a, dtype):
 
 
 def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
-              options=None, trace=False):
-    """Full V-cycle on the CPU.  Returns (part, stats_dict, events)."""
+              options=None, trace=False, prio_levels=None):
+    """Full V-cycle on the CPU.  Returns (part, stats_dict, events).
+
+    prio_levels: {level: int32[m_level]} matching priorities replacing the edge
+    weights (the learned mode); the oracle asks for every level it coarsens and
+    fails when a level or its entry count is missing."""
     lib = _load()
     rp = _as(rowptr, np.int64)
     ci = _as(colidx, np.int32)
@@ -86,9 +92,27 @@ def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
     st = GpStats()
     opt = options if isinstance(options, GpOptions) else make_options(**(options or {}))
     col = TraceCollector() if trace else None
-    rc = lib.gpo_partition(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance),
-                           int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st),
-                           C.cast(col.cfunc, C.c_void_p) if col else None, None)
+    tfn = C.cast(col.cfunc, C.c_void_p) if col else None
+    if prio_levels is None:
+        rc = lib.gpo_partition(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance),
+                               int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st), tfn, None)
+    else:
+        held = {int(l): np.ascontiguousarray(a, dtype=np.int32) for l, a in prio_levels.items()}
+        missing = []
+
+        def cb(_user, level, m):
+            a = held.get(int(level))
+            if a is None or len(a) != int(m):
+                missing.append((int(level), int(m)))
+                return None
+            return a.ctypes.data
+
+        pfn = PRIO_FN(cb)
+        rc = lib.gpo_partition_prio(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance),
+                                    int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st), tfn, None,
+                                    C.cast(pfn, C.c_void_p), None)
+        if missing:
+            raise OracleError(-1, f"no priorities for (level, m) = {missing}")
     if rc != 0:
         raise OracleError(rc, lib.gpo_last_error().decode())
     return part[:n], st.as_dict(), (col.events if col else [])

@@ -83,6 +83,12 @@ inline uint32_t loss_bucket(int32_t loss) {
 }
 
 // ------------------------------------------------------------ parameters
+// Per-level matching priorities (learned mode): prio(user, level, m) returns
+// one int32 per directed entry of that level's graph, or NULL for the edge
+// weights.  The priorities are an input here: the oracle checks that the
+// integer decisions taken from them are the same on both sides.
+typedef const int32_t* (*prio_fn_t)(void* user, int32_t level, int64_t m);
+
 struct Params {
     int32_t k;
     int64_t W;       // total vertex weight
@@ -90,6 +96,8 @@ struct Params {
     uint64_t seed;
     gp_options o;
     int64_t maxvw;   // coarse vertex weight cap
+    prio_fn_t prio = nullptr;
+    void* prio_user = nullptr;
 };
 
 void resolve_options(const gp_options* in, int64_t n, int32_t k, gp_options* o) {
@@ -158,6 +166,8 @@ int64_t max_of(const std::vector<int64_t>& a) {
 std::vector<int32_t> match_level(const Graph& g, int level, const Params& P, int* rounds_out, int64_t* pairs_out) {
     const int64_t n = g.n;
     const uint64_t salt = level_salt(P.seed, level);
+    const int32_t* pr = P.prio ? P.prio(P.prio_user, level, g.m()) : nullptr;
+    const int32_t* key_w = pr ? pr : g.ew.data();   // high word of the matching priority
     std::vector<int32_t> match(n, -1), prop(n, -1);
     int64_t pairs = 0;
     int rounds = 0;
@@ -171,7 +181,7 @@ std::vector<int32_t> match_level(const Graph& g, int level, const Params& P, int
                 int32_t u = g.ci[e];
                 if (u == v || match[u] != -1) continue;
                 if ((int64_t)g.vw[v] + g.vw[u] > P.maxvw) continue;
-                uint64_t key = edge_key(g.ew[e], edge_hash(salt, (int32_t)v, u));
+                uint64_t key = edge_key(key_w[e], edge_hash(salt, (int32_t)v, u));
                 if (best < 0 || key > bk || (key == bk && u < best)) { bk = key; best = u; }
             }
             prop[v] = best;
@@ -196,7 +206,7 @@ std::vector<int32_t> match_level(const Graph& g, int level, const Params& P, int
             for (int64_t e = g.rp[v]; e < g.rp[v + 1]; ++e) {
                 int32_t u = g.ci[e];
                 if (u == v) continue;
-                uint64_t key = edge_key(g.ew[e], edge_hash(salt, (int32_t)v, u));
+                uint64_t key = edge_key(key_w[e], edge_hash(salt, (int32_t)v, u));
                 if (best < 0 || key > bk || (key == bk && u < best)) { bk = key; best = u; }
             }
             if (best >= 0) lst.push_back({best, (int32_t)v});
@@ -621,12 +631,28 @@ int gpo_default_options(gp_options* o) {
 
 int64_t gpo_compute_lmax(int64_t W, int32_t k, float imbalance) { return compute_lmax(W, k, imbalance); }
 
+int gpo_partition_prio(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                       const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                       float imbalance, uint64_t seed, int32_t* part_out,
+                       const gp_options* opt, gp_stats* stats,
+                       gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user);
+
 // Full V-cycle on the CPU.  Same signature and semantics as gp_partition_ex.
 int gpo_partition(int64_t n, const int64_t* rowptr, const int32_t* colidx,
                   const int32_t* vwgt, const int32_t* ewgt, int32_t k,
                   float imbalance, uint64_t seed, int32_t* part_out,
                   const gp_options* opt, gp_stats* stats,
                   gp_trace_fn trace, void* trace_user) {
+    return gpo_partition_prio(n, rowptr, colidx, vwgt, ewgt, k, imbalance, seed, part_out, opt, stats, trace,
+                              trace_user, nullptr, nullptr);
+}
+
+// Same, with per-level matching priorities supplied by prio (learned mode).
+int gpo_partition_prio(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                       const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                       float imbalance, uint64_t seed, int32_t* part_out,
+                       const gp_options* opt, gp_stats* stats,
+                       gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user) {
     g_err.clear();
     if (n < 0) return fail(GP_EINVAL, "n must be >= 0");
     if (k < 1 || k > GP_MAX_K) return fail(GP_EINVAL, "k must be in [1, " + std::to_string(GP_MAX_K) + "]");
@@ -653,6 +679,7 @@ int gpo_partition(int64_t n, const int64_t* rowptr, const int32_t* colidx,
         if (vwgt) g.vw.assign(vwgt, vwgt + n);
     }
     P.k = k; P.seed = seed;
+    P.prio = prio; P.prio_user = prio_user;
     P.W = 0;
     for (int64_t v = 0; v < n; ++v) P.W += lv[0].vw[v];
     P.Lmax = compute_lmax(P.W, k, imbalance);

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 from ._abi import (
-    GpOptions, GpStats, TraceCollector, make_options, i32p, i64p, ERROR_NAMES,
+    GpOptions, GpStats, GpLearnedReport, TraceCollector, make_options, i32p, i64p, ERROR_NAMES,
 )
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -68,6 +68,32 @@ def lib():
     L.gp_partition_batch_device.argtypes = [C.c_int32, P64, P64, PP64, PP32, PP32, PP32, P32, C.POINTER(C.c_float),
                                             C.POINTER(C.c_uint64), PP32, C.c_void_p, C.c_int32,
                                             C.POINTER(GpOptions), C.POINTER(GpStats)]
+    VP = C.c_void_p
+    L.gp_gnn_num_params.restype = C.c_int
+    L.gp_gnn_create.restype = C.c_int
+    L.gp_gnn_create.argtypes = [C.POINTER(VP)]
+    L.gp_gnn_destroy.restype = C.c_int
+    L.gp_gnn_destroy.argtypes = [VP]
+    L.gp_gnn_set_params.restype = C.c_int
+    L.gp_gnn_set_params.argtypes = [VP, C.POINTER(C.c_float), C.c_int32]
+    L.gp_gnn_set_prio_bits.restype = C.c_int
+    L.gp_gnn_set_prio_bits.argtypes = [VP, C.c_int32]
+    L.gp_gnn_get_prio_bits.restype = C.c_int
+    L.gp_gnn_get_prio_bits.argtypes = [VP]
+    L.gp_gnn_get_params.restype = C.c_int
+    L.gp_gnn_get_params.argtypes = [VP, C.POINTER(C.c_float), C.c_int32]
+    L.gp_gnn_forward_device.restype = C.c_int
+    L.gp_gnn_forward_device.argtypes = [VP, C.c_int64, VP, VP, VP, VP, C.c_int32, VP, VP, VP]
+    L.gp_gnn_grad_device.restype = C.c_int
+    L.gp_gnn_grad_device.argtypes = [VP, C.c_int64, VP, VP, VP, VP, C.c_int32, VP, VP, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float)]
+    L.gp_gnn_train_step_device.restype = C.c_int
+    L.gp_gnn_train_step_device.argtypes = [VP, C.c_int32, P64, PP64, PP32, PP32, PP32, P32, C.POINTER(VP),
+                                           C.c_float, VP, C.POINTER(C.c_float)]
+    L.gp_partition_learned_device.restype = C.c_int
+    L.gp_partition_learned_device.argtypes = [C.c_int64, VP, VP, VP, VP, C.c_int32, C.c_float, C.c_uint64, VP, VP,
+                                              C.POINTER(GpOptions), C.POINTER(GpStats), VP, C.c_int32,
+                                              C.POINTER(GpLearnedReport), VP, VP]
     L.gp_default_options.restype = C.c_int
     L.gp_default_options.argtypes = [C.POINTER(GpOptions)]
     L.gp_release_workspace.restype = C.c_int
@@ -98,6 +124,12 @@ def _ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+def _collector(trace):
+    if not trace:
+        return None
+    return TraceCollector(kinds=None if trace is True else trace)
+
+
 def partition(rowptr, colidx, k: int, imbalance: float = 0.03, seed: int = 0, vwgt=None, ewgt=None,
               options=None, trace: bool = False, out=None, stream=None):
     """Partition a CSR graph into k parts.
@@ -106,11 +138,12 @@ def partition(rowptr, colidx, k: int, imbalance: float = 0.03, seed: int = 0, vw
     library copies them to the current device).  torch CUDA tensors go through
     gp_partition_device on `stream` (default: torch's current stream); the
     result is then a CUDA int32 tensor (written into `out` when given).
-    Returns (part, stats: dict, trace_events: list)."""
+    trace: True records every event; a collection of GP_TR_* kinds records
+    only those.  Returns (part, stats: dict, trace_events: list)."""
     L = lib()
     opt = _opts(options)
     st = GpStats()
-    col = TraceCollector() if trace else None
+    col = _collector(trace)
     tfn = C.cast(col.cfunc, C.c_void_p) if col else None
     seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     if _is_cuda(rowptr):
@@ -205,6 +238,147 @@ def shard_graphs(costs, world: int):
         shards[r].append(i)
         load[r] += int(costs[i])
     return shards
+
+
+class GNN:
+    """Learned edge scorer (gp_gnn handle): two message-passing layers,
+    hidden 64, BF16 weights used by every kernel, FP32 master copy and
+    accumulation.  Its only use in partitioning is the matching priority of
+    gp_partition_learned_device.  Parameters are a flat float32 array of
+    num_params() values in the layout oracle/gnn_ref.py documents."""
+
+    def __init__(self, params=None, prio_bits: int = 16):
+        self._h = C.c_void_p()
+        _check(lib().gp_gnn_create(C.byref(self._h)))
+        if params is not None:
+            self.set_params(params)
+        self.prio_bits = prio_bits
+
+    @property
+    def prio_bits(self) -> int:
+        """Resolution of the matching priority: rint(logit * 2^bits) + 2^30."""
+        return int(lib().gp_gnn_get_prio_bits(self._h))
+
+    @prio_bits.setter
+    def prio_bits(self, bits: int) -> None:
+        _check(lib().gp_gnn_set_prio_bits(self._h, int(bits)))
+
+    @staticmethod
+    def num_params() -> int:
+        return int(lib().gp_gnn_num_params())
+
+    def set_params(self, params) -> None:
+        p = np.ascontiguousarray(np.asarray(params), dtype=np.float32)
+        _check(lib().gp_gnn_set_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p)))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), dtype=np.float32)
+        _check(lib().gp_gnn_get_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p)))
+        return p
+
+    def save(self, path: str) -> None:
+        """params (float32) and prio_bits in one .npz file."""
+        with open(path, "wb") as f:
+            np.savez(f, params=self.get_params(), prio_bits=np.int32(self.prio_bits))
+
+    @classmethod
+    def load(cls, path: str) -> "GNN":
+        z = np.load(path)
+        if isinstance(z, np.ndarray):        # bare parameter array
+            return cls(z)
+        return cls(z["params"], int(z["prio_bits"]))
+
+    def forward(self, rowptr, colidx, vwgt=None, ewgt=None, level: int = 0, stream=None):
+        """(priority int32[m], logit float32[m]) CUDA tensors of one graph."""
+        import torch
+        n = rowptr.numel() - 1
+        m = colidx.numel()
+        prio = torch.empty(m, dtype=torch.int32, device=rowptr.device)
+        logit = torch.empty(m, dtype=torch.float32, device=rowptr.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+        _check(lib().gp_gnn_forward_device(self._h, n, _ptr(rowptr), _ptr(colidx), _ptr(vwgt), _ptr(ewgt), int(level),
+                                           C.c_void_p(stream), _ptr(prio), _ptr(logit)))
+        return prio, logit
+
+    def grad(self, rowptr, colidx, label, vwgt=None, ewgt=None, level: int = 0, stream=None):
+        """(mean BCE loss, gradient float32[num_params]) of one labelled graph."""
+        import torch
+        n = rowptr.numel() - 1
+        assert label.dtype == torch.uint8 and label.numel() == colidx.numel()
+        loss = C.c_float(0)
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        if stream is None:
+            stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+        _check(lib().gp_gnn_grad_device(self._h, n, _ptr(rowptr), _ptr(colidx), _ptr(vwgt), _ptr(ewgt), int(level),
+                                        _ptr(label), C.c_void_p(stream), C.byref(loss),
+                                        g.ctypes.data_as(C.POINTER(C.c_float))))
+        return float(loss.value), g
+
+    def train_step(self, samples, lr: float = 1e-3, stream=None) -> float:
+        """One Adam step over samples = [(rowptr, colidx, vwgt, ewgt, level, label)];
+        returns the mean loss before the step."""
+        import torch
+        G = len(samples)
+        ns = np.array([s[0].numel() - 1 for s in samples], dtype=np.int64)
+        vp = lambda ts: (C.c_void_p * G)(*[t.data_ptr() if t is not None else None for t in ts])
+        lv = np.array([int(s[4]) for s in samples], dtype=np.int32)
+        loss = C.c_float(0)
+        dev = samples[0][0].device
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        _check(lib().gp_gnn_train_step_device(self._h, G, i64p(ns), vp([s[0] for s in samples]),
+                                              vp([s[1] for s in samples]), vp([s[2] for s in samples]),
+                                              vp([s[3] for s in samples]), i32p(lv), vp([s[5] for s in samples]),
+                                              float(lr), C.c_void_p(stream), C.byref(loss)))
+        return float(loss.value)
+
+    def close(self) -> None:
+        if self._h:
+            lib().gp_gnn_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+WEIGHTS_PATH = os.path.join(HERE, "gnn_weights.npz")
+
+
+def default_gnn() -> GNN:
+    """The scorer trained by thegraphpartitioning_b200.learned on plain-partitioner
+    labels (gnn_weights.npz beside this file)."""
+    if not os.path.exists(WEIGHTS_PATH):
+        raise RuntimeError(f"{WEIGHTS_PATH} is missing: train it with `python -m thegraphpartitioning_b200.learned train`")
+    return GNN.load(WEIGHTS_PATH)
+
+
+def partition_learned(rowptr, colidx, k: int, model: GNN, imbalance: float = 0.03, seed: int = 0, vwgt=None,
+                      ewgt=None, options=None, judge: bool = True, trace: bool = False, out=None, stream=None):
+    """V-cycle with the model's scores as matching priorities (torch CUDA
+    tensors).  judge=True also runs the plain V-cycle and keeps the learned
+    partition only when its exact cut <= the plain cut (balance permitting).
+    Returns (part, stats, report, trace_events)."""
+    import torch
+    L = lib()
+    opt = _opts(options)
+    st = GpStats()
+    rep = GpLearnedReport()
+    col = _collector(trace)
+    tfn = C.cast(col.cfunc, C.c_void_p) if col else None
+    n = rowptr.numel() - 1
+    assert rowptr.is_cuda and rowptr.dtype == torch.int64 and colidx.dtype == torch.int32
+    part = out if out is not None else torch.empty(max(n, 0), dtype=torch.int32, device=rowptr.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+    rc = L.gp_partition_learned_device(n, _ptr(rowptr), _ptr(colidx), _ptr(vwgt), _ptr(ewgt), int(k),
+                                       float(imbalance), int(seed) & 0xFFFFFFFFFFFFFFFF, _ptr(part), C.c_void_p(stream),
+                                       C.byref(opt), C.byref(st), model._h, 1 if judge else 0, C.byref(rep), tfn, None)
+    _check(rc)
+    return part, st.as_dict(), rep.as_dict(), (col.events if col else [])
 
 
 def default_options() -> GpOptions:

@@ -23,6 +23,7 @@ GP_TR_CONTRACT = 2
 GP_TR_INITPART = 3
 GP_TR_REFINE_ITER = 4
 GP_TR_LEVEL_DONE = 5
+GP_TR_PRIO = 6
 
 ERROR_NAMES = {
     GP_EINVAL: "GP_EINVAL",
@@ -101,7 +102,26 @@ class GpTraceEvent(C.Structure):
     ]
 
 
+class GpLearnedReport(C.Structure):
+    _fields_ = [
+        ("cut_learned", C.c_int64),
+        ("cut_plain", C.c_int64),
+        ("max_part_weight_learned", C.c_int64),
+        ("max_part_weight_plain", C.c_int64),
+        ("ms_learned", C.c_double),
+        ("ms_plain", C.c_double),
+        ("ms_gnn", C.c_double),
+        ("kept_learned", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 TRACE_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(GpTraceEvent))
+# learned matching priorities handed to the oracle: (user, level, m) -> int32[m]
+PRIO_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int32, C.c_int64)
 
 
 def make_options(**kw) -> GpOptions:
@@ -137,6 +157,8 @@ def decode_event(ev: GpTraceEvent) -> dict:
         d["colidx"] = _arr(ev.colidx, m, np.int32)
         d["ewgt"] = _arr(ev.ewgt, m, np.int32)
         d["vwgt"] = _arr(ev.vwgt, n, np.int32)
+    elif ev.kind == GP_TR_PRIO:
+        d["a0"] = _arr(ev.a0, int(ev.m), np.int32)
     else:
         for name in ("a0", "a1", "a2"):
             d[name] = _arr(getattr(ev, name), n, np.int32)
@@ -147,16 +169,19 @@ class TraceCollector:
     """Callback object that stores decoded events; tracks the finer level's n
     so that the cmap of a CONTRACT event can be copied with the right length."""
 
-    def __init__(self):
+    def __init__(self, kinds=None):
         self.events: list[dict] = []
         self._last_fine_n = 0
+        self.kinds = None if kinds is None else frozenset(int(x) for x in kinds)
         self.cfunc = TRACE_FN(self._cb)
 
     def _cb(self, _user, evp):
         ev = evp.contents
-        d = decode_event(ev)
         if ev.kind == GP_TR_MATCH:
             self._last_fine_n = int(ev.n)
+        if self.kinds is not None and int(ev.kind) not in self.kinds:
+            return
+        d = decode_event(ev)
         if ev.kind == GP_TR_CONTRACT:
             d["a0"] = _arr(ev.a0, self._last_fine_n, np.int32)
         self.events.append(d)

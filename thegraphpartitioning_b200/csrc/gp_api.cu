@@ -219,8 +219,9 @@ struct Timer {
 };
 
 void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
-                int32_t* d_out, gp_stats* st, const Tracer& tr) {
+                int32_t* d_out, gp_stats* st, const Tracer& tr, const gp_gnn* gnn) {
     Params P;
+    P.gnn = gnn;
     resolve_options(opt, k, &P.o);
     P.k = k; P.seed = seed; P.imbalance = imbalance;
     Timer tm;
@@ -247,8 +248,23 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
             const int level = (int)lv.size() - 1;
             auto mk = c.tmp->save();
             int32_t* match = c.tmp_alloc<int32_t>(lv.back().g.n);
+            int32_t* prio = nullptr;
+            if (P.gnn) {
+                prio = c.tmp_alloc<int32_t>(lv.back().g.m);
+                GP_CUDA(cudaEventRecord(tm.e[4], c.s));
+                gnn_level_priorities(c, P.gnn, lv.back(), level, prio);
+                GP_CUDA(cudaEventRecord(tm.e[5], c.s));
+                if (tr.on()) {
+                    auto hp = to_host(c, prio, lv.back().g.m);
+                    gp_trace_event ev; memset(&ev, 0, sizeof ev);
+                    ev.kind = GP_TR_PRIO; ev.level = level; ev.n = lv.back().g.n; ev.m = lv.back().g.m;
+                    ev.a0 = hp.data();
+                    tr.emit(ev);
+                }
+            }
             int rounds = 0;
-            const int64_t pairs = match_level(c, lv.back(), level, P, match, &rounds);
+            const int64_t pairs = match_level(c, lv.back(), level, P, match, &rounds, prio);
+            if (P.gnn) c.ms_gnn += tm.ms(4, 5);   // match_level has synchronized the stream
             const int64_t n = lv.back().g.n;
             if (tr.on()) {
                 auto h = to_host(c, match, n);
@@ -458,6 +474,64 @@ int gp_partition_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_col
         Tracer tr; tr.fn = trace; tr.user = trace_user;
         run_vcycle(c, g, k, imbalance, seed, opt, d_part_out, stats, tr);
         c.sync();
+    });
+}
+
+int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx, const int32_t* d_vwgt,
+                                const int32_t* d_ewgt, int32_t k, float imbalance, uint64_t seed, int32_t* d_part_out,
+                                void* stream, const gp_options* opt, gp_stats* stats, const gp_gnn* model,
+                                int32_t judge, gp_learned_report* report, gp_trace_fn trace, void* trace_user) {
+    return guarded([&] {
+        check_args(n, k, imbalance);
+        if (!model) throw GpError(GP_EINVAL, "null model");
+        if (report) memset(report, 0, sizeof *report);
+        if (n == 0) { if (stats) memset(stats, 0, sizeof *stats); return; }
+        if (!d_rowptr || !d_colidx || !d_part_out) throw GpError(GP_EINVAL, "null array");
+        CallGuard G((cudaStream_t)stream);
+        Ctx& c = G.c;
+        DGraph g;
+        g.n = n;
+        g.rp = d_rowptr;
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_rowptr, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned + 1, d_rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        if (c.h_pinned[0] != 0) throw GpError(GP_EINVAL, "rowptr[0] must be 0");
+        g.m = c.h_pinned[1];
+        if (g.m < 0) throw GpError(GP_EINVAL, "rowptr[n] must be >= 0");
+        g.ci = d_colidx; g.ew = d_ewgt; g.vw = d_vwgt;
+        Tracer tr; tr.fn = trace; tr.user = trace_user;
+        gp_stats sl;
+        c.ms_gnn = 0;
+        run_vcycle(c, g, k, imbalance, seed, opt, d_part_out, &sl, tr, model);
+        c.sync();
+        gp_stats kept = sl;
+        gp_learned_report rep;
+        memset(&rep, 0, sizeof rep);
+        rep.cut_learned = sl.cut; rep.max_part_weight_learned = sl.max_part_weight; rep.ms_learned = sl.ms_total;
+        rep.ms_gnn = c.ms_gnn;
+        rep.kept_learned = 1;
+        if (judge) {
+            // the plain V-cycle into scratch; its result replaces the learned one
+            // unless the learned partition is at least as balanced (within the
+            // bound) and cuts no more
+            int32_t* plain = nullptr;
+            GP_CUDA(cudaMallocAsync(&plain, sizeof(int32_t) * n, c.s));
+            struct Free { int32_t* p; cudaStream_t s; ~Free() { cudaFreeAsync(p, s); } } fr{plain, c.s};
+            gp_stats sp;
+            Tracer none;
+            run_vcycle(c, g, k, imbalance, seed, opt, plain, &sp, none);
+            rep.cut_plain = sp.cut; rep.max_part_weight_plain = sp.max_part_weight; rep.ms_plain = sp.ms_total;
+            const bool bl = sl.max_part_weight <= sl.max_allowed, bp = sp.max_part_weight <= sp.max_allowed;
+            const bool keep_learned = (bl && !bp) || (bl == bp && sl.cut <= sp.cut);
+            rep.kept_learned = keep_learned ? 1 : 0;
+            if (!keep_learned) {
+                GP_CUDA(cudaMemcpyAsync(d_part_out, plain, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c.s));
+                kept = sp;
+            }
+            c.sync();
+        }
+        if (stats) *stats = kept;
+        if (report) *report = rep;
     });
 }
 

@@ -188,7 +188,13 @@ struct MatchArgs {
     uint64_t* keys;           // MODE 1: (anchor << nbits | v)
     int64_t* nkeys;
     int nbits;
+    const int32_t* prio;      // learned priorities per entry (nullptr: edge weights)
 };
+
+// high word of an entry's matching priority: learned score or edge weight
+__device__ __forceinline__ int32_t key_word(const MatchArgs& A, int64_t e) {
+    return A.prio ? A.prio[e] : (A.g.ew ? __ldcs(&A.g.ew[e]) : 1);
+}
 
 template <int MODE>
 __device__ __forceinline__ bool match_ok(const MatchArgs& A, int64_t v, int32_t u, int64_t vwv) {
@@ -229,7 +235,7 @@ __device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
             const int32_t u = __ldcs(&A.g.ci[e]);
             const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
             if (match_ok<MODE>(A, v, u, vwv)) {
-                bk = edge_key(A.g.ew ? __ldcs(&A.g.ew[e]) : 1, edge_hash(A.salt, (int32_t)v, u));
+                bk = edge_key(key_word(A, e), edge_hash(A.salt, (int32_t)v, u));
                 bid = u;
             }
         }
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
         for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < end; e += blockDim.x) {
             const int32_t u = __ldcs(&A.g.ci[e]);
             if (match_ok<MODE>(A, v, u, vwv))
-                argmax_merge(bk, bid, edge_key(A.g.ew ? __ldcs(&A.g.ew[e]) : 1, edge_hash(A.salt, (int32_t)v, u)), u);
+                argmax_merge(bk, bid, edge_key(key_word(A, e), edge_hash(A.salt, (int32_t)v, u)), u);
         }
         block_argmax(bk, bid, sk, sid);
         const int nit = A.row_items[h];
@@ -313,7 +319,7 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
                     for (int c = 0; c < 4; ++c) {
                         const int64_t e = base + c * 32 + lane;
                         uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-                        ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
+                        ww[c] = e < end ? key_word(A, e) : 0;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -401,7 +407,8 @@ static int bits_for(int64_t x) {  // bits to represent values in [0, x)
     return b;
 }
 
-int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out) {
+int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out,
+                    const int32_t* prio) {
     const DGraph& g = L.g;
     const uint64_t salt = level_salt(P.seed, level);
     auto mk = c.tmp->save();
@@ -419,7 +426,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     A.iid = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nitems, 1));
     A.hdone = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nheavy, 1));
     memset_async(c, A.hdone, 0, sizeof(int32_t) * std::max<int64_t>(L.nheavy, 1));
-    A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0;
+    A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0; A.prio = prio;
     for (int b = 0; b < 3; ++b) { A.list[b] = L.bucket[b]; A.nlist[b] = L.nbucket[b]; }
     int64_t pairs = 0;
     int rounds = 0;

@@ -114,6 +114,7 @@ struct Ctx {
     bool profile = false;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     double ms_conn = 0;
+    double ms_gnn = 0;            // learned mode: device time of the scorer's inference
     int64_t conn_launches = 0, conn_bytes = 0;
     template <class T> T* keep_alloc(int64_t count) { return (T*)keep->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
     template <class T> T* tmp_alloc(int64_t count) { return (T*)tmp->alloc(sizeof(T) * (size_t)(count > 0 ? count : 1)); }

@@ -9,7 +9,12 @@
 
 namespace gp {
 
+}  // namespace gp
+struct gp_gnn;   // learned edge scorer (gp_gnn.cu)
+namespace gp {
+
 struct Params {
+    const gp_gnn* gnn = nullptr;   // learned matching priorities when set
     int32_t k = 2;
     int64_t W = 0;        // total vertex weight
     int64_t Lmax = 0;     // max allowed part weight
@@ -111,7 +116,7 @@ enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NL0 = 3, S_NL1 = 4, S_
 
 // gp_api.cu
 void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
-                int32_t* d_out, gp_stats* st, const Tracer& tr);
+                int32_t* d_out, gp_stats* st, const Tracer& tr, const gp_gnn* gnn = nullptr);
 int check_args(int64_t n, int32_t k, float imbalance);
 extern thread_local std::string t_err;
 
@@ -123,9 +128,14 @@ void release_batch_workers(int dev);
 void coarsen_smem_caps();
 void initpart_smem_caps();
 
+// gp_gnn.cu
+void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, int32_t* prio);
+
 // gp_coarsen.cu
 void build_heavy(Ctx& c, Level& L);
-int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out);
+// prio: per-entry matching priority replacing the edge weight (nullptr: weights)
+int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out,
+                    const int32_t* prio = nullptr);
 void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match);
 
 // gp_initpart.cu

@@ -1,0 +1,266 @@
+"""Training and evaluation of the learned matching priorities.
+
+The reference has no code for this part (its run log names a
+GNNcoarsening.cu, script/run.txt:5-6, that is not in the repository).
+
+Data: the plain partitioner labels its own hierarchy.  For every level at
+which it matched, the level graph (the input, or a coarse graph from the
+CONTRACT trace) is one sample; an entry (v, u) is labelled 1 when v and u sit
+in the same part after that level's refinement (the LEVEL_DONE trace).  The
+network learns which edges stay inside parts; matching then contracts those
+first instead of the heaviest ones.
+
+Training runs entirely in the library's own kernels (gp_gnn_train_step_device:
+forward, backward and Adam on the GPU).  The families follow the workloads of
+the plain method: Chung-Lu power-law graphs, R-MAT, random geometric graphs
+and Erdos-Renyi graphs, n log-uniform in [2k, 64k].
+
+After training, the priority resolution (GNN.prio_bits) is chosen on a
+validation set of larger graphs from the same families (other seeds): the
+value with the lowest geometric-mean cut relative to the plain method.
+
+    python -m thegraphpartitioning_b200.learned train --graphs 2000 --out gnn_weights.npz
+    python -m thegraphpartitioning_b200.learned eval --weights gnn_weights.npz
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import GNN, partition, partition_learned, graphs as G
+from ._abi import GP_TR_MATCH, GP_TR_CONTRACT, GP_TR_LEVEL_DONE
+
+H, F0, MSG, ZD = 64, 4, 8, 4
+O_W1 = 0
+O_B1 = O_W1 + H * 2 * F0
+O_P = O_B1 + H
+O_W2 = O_P + MSG * H
+O_B2 = O_W2 + H * (H + MSG)
+O_Z = O_B2 + H
+O_A = O_Z + ZD * H
+O_BETA = O_A + ZD
+NPARAM = O_BETA + 3
+FAMILIES = ("chung_lu", "rmat", "rgg", "er")
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-scaled random weights, zero biases; the edge-weight coefficient
+    starts at 1 so that an untrained model behaves like heavy-edge matching
+    with noise."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NPARAM, dtype=np.float32)
+    p[O_W1:O_B1] = rng.normal(0, math.sqrt(2.0 / (2 * F0)), H * 2 * F0)
+    p[O_P:O_W2] = rng.normal(0, math.sqrt(1.0 / H), MSG * H)
+    p[O_W2:O_B2] = rng.normal(0, math.sqrt(2.0 / (H + MSG)), H * (H + MSG))
+    p[O_Z:O_A] = rng.normal(0, math.sqrt(1.0 / H), ZD * H)
+    p[O_A:O_BETA] = rng.normal(0, 0.1, ZD)
+    p[O_BETA] = 1.0
+    return p
+
+
+def graph_spec(i: int, seed: int = 0, nmin: int = 2000, nmax: int = 64000):
+    """Family, size, k and seed of training graph i (hash-derived)."""
+    h = G._mix64_int(G.stream_salt(seed, 7000 + i) & ((1 << 64) - 1))
+    u = (h >> 11) / float(1 << 53)
+    n = int(round(math.exp(math.log(nmin) + u * (math.log(nmax) - math.log(nmin)))))
+    fam = FAMILIES[i % len(FAMILIES)]
+    k = (2, 4, 8, 16, 32, 64)[(h >> 5) % 6]
+    return {"i": i, "family": fam, "n": n, "k": k, "seed": G._mix64_int(h ^ 0x2545F4914F6CDD1D)}
+
+
+def make_graph(spec, device="cuda"):
+    fam, n, sd = spec["family"], spec["n"], spec["seed"]
+    if fam == "chung_lu":
+        rp, ci = G.chung_lu(n, target_edges=int(3.43 * n), exponent=2.5, max_degree=max(20.0, 420.0 * n / 262111),
+                            seed=sd, device=device)
+    elif fam == "rmat":
+        scale = max(10, int(round(math.log2(n))))
+        rp, ci, _ = G.rmat(scale, 16, seed=sd, device=device)
+    elif fam == "rgg":
+        rp, ci = G.random_geometric(n, 8.0, seed=sd, device=device)
+    else:
+        rp, ci = G.erdos_renyi(n, 10.0, seed=sd, device=device)
+    return rp, ci
+
+
+def level_samples(rowptr, colidx, k: int, seed: int = 0, imbalance: float = 0.03):
+    """[(rowptr, colidx, vwgt, ewgt, level, label)] CUDA tensors for every level
+    the plain V-cycle matched at."""
+    import torch
+    dev = rowptr.device
+    _, _, ev = partition(rowptr, colidx, k, imbalance=imbalance, seed=seed,
+                         trace={GP_TR_MATCH, GP_TR_CONTRACT, GP_TR_LEVEL_DONE})
+    graphs = {0: (rowptr, colidx, None, None)}
+    parts, matched = {}, set()
+    for e in ev:
+        if e["kind"] == GP_TR_CONTRACT:
+            t = lambda a, dt: torch.from_numpy(a).to(dev, dt)
+            graphs[e["level"] + 1] = (t(e["rowptr"], torch.int64), t(e["colidx"], torch.int32),
+                                      t(e["vwgt"], torch.int32), t(e["ewgt"], torch.int32))
+        elif e["kind"] == GP_TR_LEVEL_DONE:
+            parts[e["level"]] = e["a0"]
+        elif e["kind"] == GP_TR_MATCH:
+            matched.add(e["level"])
+    out = []
+    for lvl in sorted(matched):
+        if lvl not in graphs or lvl not in parts:
+            continue
+        rp, ci, vw, ew = graphs[lvl]
+        p = torch.from_numpy(parts[lvl]).to(dev)
+        src = torch.repeat_interleave(torch.arange(rp.numel() - 1, device=dev), rp[1:] - rp[:-1])
+        label = (p[src] == p[ci.long()]).to(torch.uint8)
+        out.append((rp, ci, vw, ew, lvl, label))
+    return out
+
+
+def build_dataset(count: int, seed: int = 0, device="cuda", log=None):
+    samples, t0 = [], time.time()
+    for i in range(count):
+        spec = graph_spec(i, seed)
+        rp, ci = make_graph(spec, device)
+        n = rp.numel() - 1
+        k = min(spec["k"], max(2, n // 64))
+        samples.extend(level_samples(rp, ci, k, seed=spec["seed"]))
+        if log and (i + 1) % 200 == 0:
+            log(f"graphs {i + 1}/{count}: {len(samples)} level samples, {time.time() - t0:.1f}s")
+    return samples
+
+
+def train(model: GNN, samples, epochs: int = 4, batch: int = 32, lr: float = 3e-3, seed: int = 0, log=None):
+    """Adam over shuffled mini-batches; cosine-decayed step size.  Returns the
+    mean loss of each epoch."""
+    rng = np.random.default_rng(seed)
+    steps = epochs * ((len(samples) + batch - 1) // batch)
+    step, hist = 0, []
+    for ep in range(epochs):
+        order = rng.permutation(len(samples))
+        tot, cnt = 0.0, 0
+        for b in range(0, len(order), batch):
+            cur = lr * 0.5 * (1 + math.cos(math.pi * step / max(steps, 1)))
+            loss = model.train_step([samples[j] for j in order[b:b + batch]], lr=max(cur, lr * 0.02))
+            tot += loss
+            cnt += 1
+            step += 1
+        hist.append(tot / max(cnt, 1))
+        if log:
+            log(f"epoch {ep}: mean loss {hist[-1]:.4f}")
+    return hist
+
+
+def validation_set(count_per_family: int = 2, seed: int = 1, n: int = 200_000, device="cuda"):
+    """Larger graphs of the training families (other seeds) for choosing prio_bits."""
+    out = []
+    for j in range(count_per_family * len(FAMILIES)):
+        spec = graph_spec(j, seed, nmin=n, nmax=n)
+        spec["family"] = FAMILIES[j % len(FAMILIES)]
+        out.append(make_graph(spec, device))
+    return out
+
+
+def tune_prio_bits(model: GNN, graphs, k: int = 32, candidates=(4, 6, 8, 10, 12, 16), log=None):
+    """Set model.prio_bits to the candidate with the lowest geometric-mean
+    learned/plain cut ratio over `graphs`; returns {bits: ratio}."""
+    plain = [partition(rp, ci, k)[1]["cut"] for rp, ci in graphs]
+    res = {}
+    for b in candidates:
+        model.prio_bits = b
+        logs = [math.log(max(partition_learned(rp, ci, k, model, judge=False)[1]["cut"], 1) / max(c, 1))
+                for (rp, ci), c in zip(graphs, plain)]
+        res[b] = math.exp(sum(logs) / len(logs))
+        if log:
+            log(f"prio_bits {b}: geometric-mean cut ratio {res[b]:.4f}")
+    model.prio_bits = min(res, key=lambda b: (res[b], -b))
+    return res
+
+
+def evaluate(model: GNN, rowptr, colidx, k: int, seed: int = 0, imbalance: float = 0.03, reps: int = 1):
+    """Plain vs learned V-cycle on one graph: cuts, balance and device times
+    (one untimed warm-up of each, then the fastest of `reps` runs)."""
+    import torch
+    partition(rowptr, colidx, k, imbalance=imbalance, seed=seed)
+    partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, judge=False)
+    best = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        _, sp, _ = partition(rowptr, colidx, k, imbalance=imbalance, seed=seed)
+        _, sl, rep, _ = partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, judge=False)
+        r = {"cut_plain": sp["cut"], "cut_learned": sl["cut"], "imb_plain": sp["imbalance"],
+             "imb_learned": sl["imbalance"], "ms_plain": sp["ms_total"], "ms_learned": sl["ms_total"],
+             "ms_gnn": rep["ms_gnn"], "balanced_learned": sl["max_part_weight"] <= sl["max_allowed"]}
+        for key in ("ms_coarsen", "ms_initial", "ms_refine", "levels", "refine_iters"):
+            r[key + "_plain"], r[key + "_learned"] = sp[key], sl[key]
+        if best is None or r["ms_learned"] < best["ms_learned"]:
+            best = r
+    best["cut_ratio"] = best["cut_learned"] / max(best["cut_plain"], 1)
+    best["time_ratio"] = best["ms_learned"] / max(best["ms_plain"], 1e-9)
+    return best
+
+
+def held_out(name: str, device="cuda"):
+    """The evaluation graphs: R-MAT scale 22 and the 3D 7-point grid 256^3."""
+    if name == "rmat22":
+        rp, ci, _ = G.rmat(22, 16, seed=12345, device=device)
+        return rp, ci
+    if name == "grid3d256":
+        return G.grid3d(256, 256, 256, device=device)
+    raise KeyError(name)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--graphs", type=int, default=2000)
+    t.add_argument("--epochs", type=int, default=4)
+    t.add_argument("--batch", type=int, default=32)
+    t.add_argument("--lr", type=float, default=3e-3)
+    t.add_argument("--seed", type=int, default=0)
+    t.add_argument("--out", default="gnn_weights.npz")
+    t.add_argument("--init", default=None, help="start from these weights instead of a seeded init")
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", default=None)
+    e.add_argument("--graphs", default="rmat22,grid3d256")
+    e.add_argument("--k", type=int, default=32)
+    e.add_argument("--reps", type=int, default=2)
+    e.add_argument("--json", default=None)
+    a = ap.parse_args(argv)
+    log = lambda s: print(s, flush=True)
+    import torch
+    if a.cmd == "train":
+        t0 = time.time()
+        samples = build_dataset(a.graphs, a.seed, log=log)
+        log(f"dataset: {len(samples)} samples, {sum(int(s[1].numel()) for s in samples)} entries, "
+            f"{time.time() - t0:.1f}s")
+        model = GNN.load(a.init) if a.init else GNN(init_params(a.seed))
+        t1 = time.time()
+        hist = train(model, samples, a.epochs, a.batch, a.lr, a.seed, log=log)
+        log(f"training: {time.time() - t1:.1f}s, loss {hist[0]:.4f} -> {hist[-1]:.4f}")
+        del samples
+        torch.cuda.empty_cache()
+        tune_prio_bits(model, validation_set(), log=log)
+        log(f"prio_bits = {model.prio_bits}")
+        model.save(a.out)
+        log(f"saved {a.out}")
+    else:
+        from . import default_gnn
+        model = GNN.load(a.weights) if a.weights else default_gnn()
+        res = {}
+        for name in a.graphs.split(","):
+            rp, ci = held_out(name)
+            r = evaluate(model, rp, ci, a.k, reps=a.reps)
+            r.update({"graph": name, "n": rp.numel() - 1, "undirected_edges": ci.numel() // 2, "k": a.k})
+            log(json.dumps(r))
+            res[name] = r
+            del rp, ci
+            torch.cuda.empty_cache()
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(res, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
