@@ -67,7 +67,12 @@ typedef struct gp_options {
     int32_t check_input;        /* 0/1: structural checks, 2: +symmetry, <0: none        */
     int32_t verbose;            /* 0: silent                                           */
     int32_t profile;            /* 1: time the connectivity pass with CUDA events       */
-    int32_t reserved[4];
+    int32_t small_level_n;      /* > 0: refine levels of at most this many vertices
+                                   (capped at 16384) without rows above 2048 entries in
+                                   one thread block, one launch per level; 0 or < 0:
+                                   off.  Results are identical either way; it pays
+                                   only where launches, not SMs, are scarce            */
+    int32_t reserved[3];
 } gp_options;
 
 /* Result record of one call. */

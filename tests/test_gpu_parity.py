@@ -30,6 +30,17 @@ def _cases():
     yield "rmat11_k64_tight", graphs.rmat(11, seed=3)[:2], 64, 0.0, None, {}
     yield "er_k3_nohop", graphs.erdos_renyi(3000, 3.0, seed=5), 3, 0.02, None, {"two_hop": -1}
     yield "rgg_k2", graphs.random_geometric(4000, 8.0, seed=6), 2, 0.03, None, {"init_trials": 8}
+    # the same workloads with every level refined by the multi-kernel loop, or
+    # with a mix of both paths (small_level_n: levels above it multi-kernel)
+    yield "rmat12_k16_multikernel", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"small_level_n": -1}
+    yield "grid3d_k32_multikernel", graphs.grid3d(16, 16, 16), 32, 0.03, None, {"small_level_n": -1}
+    yield "weighted_k5_mixed", graphs.grid2d(40, 50), 5, 0.05, "w", {"small_level_n": 1200}
+    yield "chunglu_k8_mixed", graphs.chung_lu(12000, 40000, seed=2), 8, 0.03, None, {"small_level_n": 3000}
+    yield "er_k64_cta", graphs.erdos_renyi(16000, 8.0, seed=8), 64, 0.03, None, {"small_level_n": 16384}
+    # exact balance on 50k-60k vertices: rebalance steps with more candidates
+    # than one thread block sorts (radix-sorted multi-kernel path), weak and strong
+    yield "rgg50k_k2_bigrb", graphs.random_geometric(50000, 8.0, seed=9), 2, 0.0, None, {}
+    yield "er60k_k3_bigrb", graphs.erdos_renyi(60000, 10.0, seed=3), 3, 0.0, None, {}
 
 
 CASES = list(_cases())

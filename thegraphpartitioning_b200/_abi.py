@@ -48,7 +48,8 @@ class GpOptions(C.Structure):
         ("check_input", C.c_int32),
         ("verbose", C.c_int32),
         ("profile", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("small_level_n", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

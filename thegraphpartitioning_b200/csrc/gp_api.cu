@@ -42,6 +42,7 @@ void ensure_kernel_caps(int dev) {
     std::lock_guard<std::mutex> lk(mu);
     if (done[dev]) return;
     coarsen_smem_caps();
+    refine_smem_caps();
     initpart_smem_caps();
     done[dev] = true;
 }

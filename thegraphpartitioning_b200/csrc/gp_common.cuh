@@ -71,6 +71,38 @@ __host__ __device__ __forceinline__ uint32_t mag_bucket(uint32_t x) {
     uint32_t mant = (x >> (e - 4)) & 15u;
     return 64u + (uint32_t)(e - 6) * 16u + mant;
 }
+template <class T>
+__device__ __forceinline__ T warp_incl_scan(T x) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// block-wide exclusive scan of one value per thread; sh_warp holds 33 values;
+// returns the block total in `total`
+template <class T>
+__device__ __forceinline__ T block_excl_scan(T x, T* sh_warp, T& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T inc = warp_incl_scan(x);
+    if (lane == 31) sh_warp[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        T s = lane < nw ? sh_warp[lane] : T(0);
+        T si = warp_incl_scan(s);
+        if (lane < nw) sh_warp[lane] = si - s;
+        if (lane == nw - 1) sh_warp[32] = si;
+    }
+    __syncthreads();
+    T r = inc - x + sh_warp[w];
+    total = sh_warp[32];
+    __syncthreads();
+    return r;
+}
+
 __host__ __device__ __forceinline__ uint32_t loss_bucket(int32_t loss) {
     if (loss >= 0) return 480u + mag_bucket((uint32_t)loss);
     return 480u - mag_bucket((uint32_t)(-(int64_t)loss));

@@ -126,6 +126,7 @@ void ensure_kernel_caps(int dev);   // once per device, before any launch
 void release_batch_workers(int dev);
 // per-file shared-memory caps (gp_coarsen.cu, gp_initpart.cu)
 void coarsen_smem_caps();
+void refine_smem_caps();
 void initpart_smem_caps();
 
 // gp_gnn.cu

@@ -104,37 +104,6 @@ constexpr int SCAN_T = 256;
 constexpr int SCAN_I = 8;
 constexpr int SCAN_TILE = SCAN_T * SCAN_I;
 
-template <class T>
-__device__ __forceinline__ T warp_incl_scan(T x) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    return x;
-}
-
-// block-wide exclusive scan of one value per thread; returns the block total
-template <class T>
-__device__ __forceinline__ T block_excl_scan(T x, T* sh_warp, T& total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    T inc = warp_incl_scan(x);
-    if (lane == 31) sh_warp[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        T s = lane < nw ? sh_warp[lane] : T(0);
-        T si = warp_incl_scan(s);
-        if (lane < nw) sh_warp[lane] = si - s;
-        if (lane == nw - 1) sh_warp[32] = si;
-    }
-    __syncthreads();
-    T r = inc - x + sh_warp[w];
-    total = sh_warp[32];
-    __syncthreads();
-    return r;
-}
-
 template <class TI, class TO>
 __global__ void k_tile_reduce(const TI* __restrict__ in, int64_t n, TO* __restrict__ tile_sums) {
     __shared__ TO sh[33];

@@ -475,6 +475,40 @@ __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* 
     if (tl == 0 && v >= 0 && t >= 0) ab_commit(A, v, p, d, delta, moves);
 }
 
+// one candidate row of 33..kHeavyDeg entries per warp, 128 entries per sweep
+__device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
+    const int lane = threadIdx.x & 31;
+    const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
+    const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
+    int32_t g2 = 0;
+    for (int64_t base = beg; base < end; base += 128) {
+        int32_t uu[4], ww[4], pu[4], du[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t e = base + c * 32 + lane;
+            uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
+            ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            pu[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
+            du[c] = uu[c] >= 0 ? A.dest[uu[c]] : -1;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (uu[c] < 0) continue;
+            int32_t q = pu[c];
+            if (du[c] >= 0) {
+                const int32_t gu = A.gain[uu[c]];
+                if (gu > gv || (gu == gv && uu[c] < (int32_t)v)) q = du[c];
+            }
+            g2 += q == d ? ww[c] : (q == p ? -ww[c] : 0);
+        }
+    }
+    g2 = warp_sum(g2);
+    if (lane == 0 && g2 >= 0) ab_commit(A, v, p, d, delta, moves);
+}
+
 __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
     extern __shared__ int64_t delta[];
     __shared__ int64_t s_red[RW];
@@ -525,36 +559,7 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
             } else if (u < U0 + n1) {
                 ab_tile<kTile32>(A, A.clist[1][u - U0], delta, moves);
             } else {
-                const int64_t v = A.clist[2][u - U0 - n1];
-                const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
-                const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
-                int32_t g2 = 0;
-                for (int64_t base = beg; base < end; base += 128) {
-                    int32_t uu[4], ww[4], pu[4], du[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const int64_t e = base + c * 32 + lane;
-                        uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-                        ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
-                    }
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        pu[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
-                        du[c] = uu[c] >= 0 ? A.dest[uu[c]] : -1;
-                    }
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        if (uu[c] < 0) continue;
-                        int32_t q = pu[c];
-                        if (du[c] >= 0) {
-                            const int32_t gu = A.gain[uu[c]];
-                            if (gu > gv || (gu == gv && uu[c] < (int32_t)v)) q = du[c];
-                        }
-                        g2 += q == d ? ww[c] : (q == p ? -ww[c] : 0);
-                    }
-                }
-                g2 = warp_sum(g2);
-                if (lane == 0 && g2 >= 0) ab_commit(A, v, p, d, delta, moves);
+                ab_warp(A, A.clist[2][u - U0 - n1], delta, moves);
             }
         }
     }
@@ -750,6 +755,449 @@ void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, in
     if (d_pw) part_weights(c, g, part, k, d_pw);
 }
 
+// ------------------------------------------------------------------ one-CTA refinement
+// A level with at most small_level_n (<= kCtaMaxN) vertices and no row longer
+// than kHeavyDeg is refined by one thread block in one launch: the whole
+// iteration loop of refine_level (connectivity pass, label propagation with
+// afterburner, weak/strong rebalancing, best-state tracking and the stop
+// rules) runs on the device, with the same per-row helpers as the
+// multi-kernel path and the same integer results.  Rebalance candidates are
+// sorted by a bitonic network in shared memory on unique 64-bit keys
+// (source, loss bucket, id), then (destination, loss bucket, source, id).
+constexpr int CT = 1024, CW = CT / 32;
+constexpr int64_t kCtaMaxN = 16384;                 // candidates sorted in shared memory (8 B each)
+
+struct CtaRefineArgs {
+    DGraph g;
+    int32_t k;
+    int64_t Lmax;
+    int32_t den, max_iters, patience, strong_after;
+    const int32_t* bucket[3];
+    int64_t nbucket[3];
+    int32_t* part;
+    int32_t* part_next;
+    uint8_t* lock;
+    uint8_t* lock_next;
+    int32_t* best;
+    int64_t* pw;          // in: part weights of part; out: those of the kept state
+    int32_t* dest;
+    int32_t* gain;
+    int64_t* status;      // counters of the per-row helpers
+    int32_t* clist[3];
+    int64_t* pre;         // n scratch
+    int32_t* flag;        // n scratch
+    uint64_t* gkeys;      // n scratch
+    int32_t* tr_arrays;   // optional: per step dest[n], gain[n], part[n]
+    int64_t* tr_scalars;  // optional: per step mode, cut before, max part weight before, moves
+    int64_t* out;         // [0] steps
+};
+
+__device__ __forceinline__ int64_t cta_sum(int64_t x, int64_t* sh) {
+    int64_t tot;
+    block_excl_scan<int64_t>(x, sh, tot);
+    return tot;
+}
+
+// exclusive prefix sums of val(i), i < cnt, in index order into out; returns the total
+template <class F>
+__device__ int64_t cta_scan(int64_t cnt, F val, int64_t* out, int64_t* sh) {
+    const int64_t per = (cnt + CT - 1) / CT;
+    const int64_t b = (int64_t)threadIdx.x * per, e = b + per < cnt ? b + per : cnt;
+    int64_t s = 0;
+    for (int64_t i = b; i < e; ++i) s += val(i);
+    int64_t tot;
+    int64_t base = block_excl_scan<int64_t>(s, sh, tot);
+    for (int64_t i = b; i < e; ++i) { const int64_t x = val(i); out[i] = base; base += x; }
+    __syncthreads();
+    return tot;
+}
+
+// ascending bitonic sort of N (a power of two) unique keys in shared memory
+__device__ void cta_bitonic(uint64_t* a, int N) {
+    for (int size = 2; size <= N; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < N; i += CT) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const uint64_t x = a[i], y = a[j];
+                    const bool up = (i & size) == 0;
+                    if ((x > y) == up) { a[i] = y; a[j] = x; }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+// first index in [0, i] whose key has the same segment (key >> shift) as key i
+__device__ __forceinline__ int cta_seg_start(const uint64_t* a, int i, int shift) {
+    const uint64_t seg = a[i] >> shift;
+    int lo = 0, hi = i;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((a[mid] >> shift) < seg) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// One rebalance step by one thread block (the rules of the multi-kernel path
+// below: candidates ordered (source, loss bucket, id); a source keeps the
+// prefix before the vertex below its excess; weak: per destination, ordered
+// (destination, loss bucket, source, id), moves that fit the remaining
+// capacity; strong: kept moves laid over the concatenated free capacities).
+// cand: the candidates in vertex order (ncand of them), or nullptr to take
+// every v < n with dest[v] >= 0.  s_pw (shared) is updated; returns this
+// thread's move count.  Needs ncand <= kCtaMaxN.
+struct RbCta {
+    const int32_t* vw;
+    int32_t* part;
+    uint8_t* lock;
+    const int32_t* dest;
+    const int32_t* gain;
+    int64_t* pre;
+    int32_t* flag;
+    uint64_t* gkeys;
+    int32_t k;
+    int64_t Lmax;
+};
+
+__device__ int64_t cta_rebalance(const RbCta& R, int mode, int64_t n, const int32_t* cand, int64_t ncand_in,
+                                 int64_t* s_pw, int64_t* s_snap, int64_t* s_cum, uint64_t* s_keys, int64_t* sh) {
+    const int32_t k = R.k;
+    const int64_t Lmax = R.Lmax;
+    int32_t* part = R.part;
+    uint8_t* lock = R.lock;
+    int64_t moves = 0;
+    for (int q = threadIdx.x; q < k; q += CT) s_snap[q] = s_pw[q];
+    __syncthreads();
+    int64_t ncand = ncand_in;
+    auto key1 = [&](uint32_t v) -> uint64_t {
+        const uint64_t key = ((uint64_t)(uint32_t)part[v] << RB_SHIFT) | loss_bucket(-R.gain[v]);
+        return (key << 32) | v;
+    };
+    if (cand == nullptr) {
+        // candidates in vertex order, then sorted by (source, loss bucket, id)
+        ncand = cta_scan(n, [&](int64_t v) -> int64_t { return R.dest[v] >= 0 ? 1 : 0; }, R.pre, sh);
+        for (int64_t v = threadIdx.x; v < n; v += CT)
+            if (R.dest[v] >= 0) s_keys[R.pre[v]] = key1((uint32_t)v);
+    } else {
+        for (int64_t i = threadIdx.x; i < ncand; i += CT) s_keys[i] = key1((uint32_t)cand[i]);
+    }
+    int N = 1;
+    while (N < ncand) N <<= 1;
+    for (int64_t i = ncand + threadIdx.x; i < N; i += CT) s_keys[i] = ~0ull;
+    __syncthreads();
+    cta_bitonic(s_keys, N);
+    auto vwt = [&](uint32_t v) -> int64_t { return R.vw ? R.vw[v] : 1; };
+    cta_scan(ncand, [&](int64_t i) -> int64_t { return vwt((uint32_t)s_keys[i]); }, R.pre, sh);
+    // kept: the source's prefix before the vertex is below its excess
+    for (int64_t i = threadIdx.x; i < ncand; i += CT) {
+        const uint32_t src = (uint32_t)(s_keys[i] >> (32 + RB_SHIFT));
+        const int s0 = cta_seg_start(s_keys, (int)i, 32 + RB_SHIFT);
+        R.flag[i] = (R.pre[i] - R.pre[s0]) < (s_snap[src] - Lmax) ? 1 : 0;
+    }
+    __syncthreads();
+    if (mode == 1) {
+        // kept moves re-keyed (dest, loss bucket, source, id): 10 + 10 + 10 + 32 bits
+        const int64_t n2 = cta_scan(ncand, [&](int64_t i) -> int64_t { return R.flag[i]; }, R.pre, sh);
+        for (int64_t i = threadIdx.x; i < ncand; i += CT)
+            if (R.flag[i]) {
+                const uint64_t key = s_keys[i];
+                const uint32_t v = (uint32_t)key, b = (uint32_t)(key >> 32) & ((1u << RB_SHIFT) - 1);
+                const uint32_t src = (uint32_t)(key >> (32 + RB_SHIFT));
+                R.gkeys[R.pre[i]] = ((((uint64_t)(uint32_t)R.dest[v] << RB_SHIFT | b) << RB_SHIFT | src) << 32) | v;
+            }
+        __syncthreads();
+        int N2 = 1;
+        while (N2 < n2) N2 <<= 1;
+        for (int64_t i = threadIdx.x; i < N2; i += CT) s_keys[i] = i < n2 ? R.gkeys[i] : ~0ull;
+        __syncthreads();
+        cta_bitonic(s_keys, N2);
+        cta_scan(n2, [&](int64_t i) -> int64_t { return vwt((uint32_t)s_keys[i]); }, R.pre, sh);
+        for (int64_t i = threadIdx.x; i < n2; i += CT) {
+            const uint32_t v = (uint32_t)s_keys[i];
+            const int32_t d = (int32_t)(s_keys[i] >> (32 + 2 * RB_SHIFT));
+            const int s0 = cta_seg_start(s_keys, (int)i, 32 + 2 * RB_SHIFT);
+            const int64_t wv = vwt(v);
+            if ((R.pre[i] - R.pre[s0]) + wv <= Lmax - s_snap[d]) {
+                const int32_t p = part[v];
+                part[v] = d; lock[v] = 1;
+                atomicAdd((unsigned long long*)&s_pw[d], (unsigned long long)wv);
+                atomicAdd((unsigned long long*)&s_pw[p], (unsigned long long)(-wv));
+                ++moves;
+            }
+        }
+    } else {
+        // free capacities of the parts within Lmax, concatenated (k <= CT)
+        {
+            const int64_t f = (threadIdx.x < k && s_snap[threadIdx.x] <= Lmax) ? Lmax - s_snap[threadIdx.x] : 0;
+            int64_t tot;
+            const int64_t ex = block_excl_scan<int64_t>(f, sh, tot);
+            if (threadIdx.x < k) s_cum[threadIdx.x] = ex;
+            if (threadIdx.x == 0) s_cum[k] = tot;
+            __syncthreads();
+        }
+        cta_scan(ncand, [&](int64_t i) -> int64_t { return R.flag[i] ? vwt((uint32_t)s_keys[i]) : 0; }, R.pre, sh);
+        for (int64_t i = threadIdx.x; i < ncand; i += CT) {
+            if (!R.flag[i]) continue;
+            const int64_t pre = R.pre[i];
+            if (pre >= s_cum[k]) continue;
+            int lo = 0, hi = k;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_cum[mid] <= pre) lo = mid; else hi = mid - 1;
+            }
+            const uint32_t v = (uint32_t)s_keys[i];
+            const int64_t wv = vwt(v);
+            if (lo < k && pre + wv <= s_cum[lo + 1]) {
+                const int32_t p = part[v];
+                part[v] = lo; lock[v] = 1;
+                atomicAdd((unsigned long long*)&s_pw[lo], (unsigned long long)wv);
+                atomicAdd((unsigned long long*)&s_pw[p], (unsigned long long)(-wv));
+                ++moves;
+            }
+        }
+    }
+    __syncthreads();
+    return moves;
+}
+
+// one rebalance step of the multi-kernel loop in one launch: candidates from
+// dest (n <= kCtaMaxN, locks cleared here) or from a compacted list; part
+// weights in and out of global memory; the step's moves added to *moves_out
+__global__ void __launch_bounds__(CT, 1) k_rb_step_cta(RbCta R, int mode, int64_t n, const int32_t* cand,
+                                                        int64_t ncand, int64_t* pw, int64_t* moves_out) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    const int32_t k = R.k;
+    int64_t* s_pw = (int64_t*)rsm;
+    int64_t* s_snap = s_pw + k;
+    int64_t* s_cum = s_snap + 2 * k;
+    uint64_t* s_keys = (uint64_t*)(rsm + (((size_t)(4 * k + 1) * 8 + k + 15) & ~(size_t)15));
+    __shared__ int64_t sh[33];
+    for (int q = threadIdx.x; q < k; q += CT) s_pw[q] = pw[q];
+    if (cand == nullptr)
+        for (int64_t v = threadIdx.x; v < n; v += CT) R.lock[v] = 0;
+    __syncthreads();
+    const int64_t moves = cta_sum(cta_rebalance(R, mode, n, cand, ncand, s_pw, s_snap, s_cum, s_keys, sh), sh);
+    for (int q = threadIdx.x; q < k; q += CT) pw[q] = s_pw[q];
+    if (threadIdx.x == 0) *moves_out += moves;
+}
+
+__global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    const int32_t k = R.k;
+    const int64_t Lmax = R.Lmax, n = R.g.n;
+    int64_t* s_pw = (int64_t*)rsm;               // k: current part weights
+    int64_t* s_snap = s_pw + k;                  // k: weights at the start of a rebalance step
+    int64_t* s_best = s_snap + k;                // k: weights of the kept state
+    int64_t* s_cum = s_best + k;                 // k + 1: free capacity prefix (strong)
+    uint8_t* s_over = (uint8_t*)(s_cum + k + 1); // k
+    unsigned char* big = rsm + (((size_t)(4 * k + 1) * 8 + k + 15) & ~(size_t)15);
+    int32_t* s_hist = (int32_t*)big;             // CW * k connectivity histograms, or
+    uint64_t* s_keys = (uint64_t*)big;           // up to kCtaMaxN sort keys
+    __shared__ int64_t sh[33];
+    __shared__ uint64_t s_lk[CW];
+    __shared__ int32_t s_lq[CW];
+    __shared__ int64_t s_mx[CW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t* part = R.part;
+    int32_t* part_next = R.part_next;
+    uint8_t* lock = R.lock;
+    uint8_t* lock_next = R.lock_next;
+    for (int q = threadIdx.x; q < k; q += CT) s_pw[q] = R.pw[q];
+    for (int64_t v = threadIdx.x; v < n; v += CT) lock[v] = 0;
+    __syncthreads();
+    int64_t best_cut = 0, best_mp = 0, prev_moves = -1, nmoves = 0;
+    int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
+    const int64_t U2 = R.nbucket[2], U1 = R.nbucket[1], U0 = (R.nbucket[0] + 3) / 4;
+    for (int it = 0;; ++it) {
+        const bool final_eval = it == R.max_iters;
+        // ---- part-weight summary (as k_conn's prologue)
+        int64_t mx = 0;
+        uint64_t lk = 0; int32_t lq = -1;
+        for (int q = threadIdx.x; q < k; q += CT) {
+            const int64_t x = s_pw[q];
+            s_over[q] = x > Lmax;
+            mx = x > mx ? x : mx;
+            if (x <= Lmax) argmax_q(lk, lq, ~(uint64_t)x, q);
+        }
+        for (int i = threadIdx.x; i < CW * k; i += CT) s_hist[i] = 0;
+        if (threadIdx.x < S_NRESET) R.status[threadIdx.x] = 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) { const int64_t y = __shfl_xor_sync(0xffffffffu, mx, o); mx = y > mx ? y : mx; }
+        warp_argmax_q(lk, lq);
+        if (lane == 0) { s_mx[w] = mx; s_lk[w] = lk; s_lq[w] = lq; }
+        __syncthreads();
+        int64_t maxpw = 0; uint64_t lk2 = 0; int32_t light = -1;
+        for (int i = 0; i < CW; ++i) { maxpw = s_mx[i] > maxpw ? s_mx[i] : maxpw; argmax_q(lk2, light, s_lk[i], s_lq[i]); }
+        const int dmode = final_eval ? MODE_EVAL : (maxpw > Lmax ? MODE_RB : MODE_LP);
+        // ---- connectivity pass
+        ConnArgs CA;
+        CA.g = R.g; CA.k = k; CA.Lmax = Lmax; CA.den = R.den; CA.force_eval = final_eval ? 1 : 0;
+        CA.part = part; CA.lock = lock; CA.pw = s_pw; CA.heavy = nullptr; CA.item_row = nullptr;
+        CA.item_beg = nullptr; CA.item_end = nullptr; CA.row_items = nullptr; CA.nitems = 0;
+        for (int b = 0; b < 3; ++b) { CA.bucket[b] = R.bucket[b]; CA.nbucket[b] = R.nbucket[b]; CA.clist[b] = R.clist[b]; }
+        CA.unit_cost = nullptr; CA.nunits = 0;
+        CA.dest = R.dest; CA.gain = R.gain; CA.status = R.status;
+        CA.hhist = nullptr; CA.hsum = nullptr; CA.hdone = nullptr;
+        int64_t acc = 0;
+        int32_t* hist = s_hist + w * k;
+        for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
+            if (u < U2) conn_warp(CA, R.bucket[2][u], dmode, s_over, light, hist, acc);
+            else if (u < U2 + U1) conn_tile<kTile32>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, acc);
+            else {
+                const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
+                conn_tile<kTile8>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, acc);
+            }
+        }
+        acc = warp_sum(acc);
+        const int64_t cur_cut = cta_sum(lane == 0 ? acc : 0, sh) / 2;   // also orders the pass
+        const int64_t cur_mp = maxpw;
+        // ---- best state and stop rules (every thread holds the same values)
+        if (it == 0) {
+            best_cut = cur_cut; best_mp = cur_mp;
+            for (int64_t v = threadIdx.x; v < n; v += CT) R.best[v] = part[v];
+            for (int q = threadIdx.x; q < k; q += CT) s_best[q] = s_pw[q];
+        } else {
+            const bool cb = cur_mp <= Lmax, bb = best_mp <= Lmax;
+            bool better = false, signif = false;
+            if (cb && !bb) { better = true; signif = true; }
+            else if (cb && bb) { better = cur_cut < best_cut; signif = 1000 * cur_cut < 999 * best_cut; }
+            else if (!cb && !bb) { better = cur_mp < best_mp || (cur_mp == best_mp && cur_cut < best_cut); signif = cur_mp < best_mp; }
+            if (better) {
+                best_cut = cur_cut; best_mp = cur_mp;
+                for (int64_t v = threadIdx.x; v < n; v += CT) R.best[v] = part[v];
+                for (int q = threadIdx.x; q < k; q += CT) s_best[q] = s_pw[q];
+            }
+            stall = signif ? 0 : stall + 1;
+            const bool lp_idle = (last_mode == 0 && nmoves == 0 && prev_moves == 0);
+            prev_moves = nmoves;
+            bool rb_stuck = false;
+            if (last_mode != 0 && nmoves == 0) {
+                if (last_mode == 1) rb_streak = R.strong_after; else rb_stuck = true;
+            }
+            if (stall >= R.patience || lp_idle || rb_stuck) break;
+        }
+        if (final_eval) break;
+        int mode;
+        if (dmode == MODE_RB) { mode = (rb_streak >= R.strong_after) ? 2 : 1; ++rb_streak; }
+        else { mode = 0; rb_streak = 0; }
+        last_mode = mode;
+        int64_t moves = 0;
+        __syncthreads();
+        if (mode == 0) {
+            for (int64_t v = threadIdx.x; v < n; v += CT) { part_next[v] = part[v]; lock_next[v] = 0; }
+            __syncthreads();
+            ApplyArgs AA;
+            AA.g = R.g; AA.k = k; AA.part = part; AA.dest = R.dest; AA.gain = R.gain; AA.heavy = nullptr;
+            AA.item_row = nullptr; AA.item_beg = nullptr; AA.item_end = nullptr; AA.row_items = nullptr; AA.nitems = 0;
+            for (int b = 0; b < 3; ++b) AA.clist[b] = R.clist[b];
+            AA.status = R.status; AA.part_next = part_next; AA.lock_next = lock_next; AA.pw = nullptr;
+            AA.moves_out = nullptr; AA.hsum = nullptr; AA.hdone = nullptr;
+            for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
+                if (u < U2) {
+                    const int64_t v = R.bucket[2][u];
+                    if (R.dest[v] >= 0) ab_warp(AA, v, s_pw, moves);
+                } else if (u < U2 + U1) {
+                    const int64_t v = R.bucket[1][u - U2];
+                    ab_tile<kTile32>(AA, R.dest[v] >= 0 ? v : -1, s_pw, moves);
+                } else {
+                    const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
+                    const int64_t v = i < R.nbucket[0] ? R.bucket[0][i] : -1;
+                    ab_tile<kTile8>(AA, (v >= 0 && R.dest[v] >= 0) ? v : -1, s_pw, moves);
+                }
+            }
+            nmoves = cta_sum(moves, sh);
+            int32_t* tp = part; part = part_next; part_next = tp;
+            uint8_t* tl = lock; lock = lock_next; lock_next = tl;
+        } else {
+            for (int64_t v = threadIdx.x; v < n; v += CT) lock[v] = 0;
+            __syncthreads();
+            RbCta RA;
+            RA.vw = R.g.vw; RA.part = part; RA.lock = lock; RA.dest = R.dest; RA.gain = R.gain; RA.pre = R.pre;
+            RA.flag = R.flag; RA.gkeys = R.gkeys; RA.k = k; RA.Lmax = Lmax;
+            moves = cta_rebalance(RA, mode, n, nullptr, 0, s_pw, s_snap, s_cum, s_keys, sh);
+            nmoves = cta_sum(moves, sh);
+        }
+        if (R.tr_arrays) {
+            int32_t* t = R.tr_arrays + (int64_t)steps * 3 * n;
+            for (int64_t v = threadIdx.x; v < n; v += CT) { t[v] = R.dest[v]; t[n + v] = R.gain[v]; t[2 * n + v] = part[v]; }
+            if (threadIdx.x == 0) {
+                int64_t* sc = R.tr_scalars + 4 * steps;
+                sc[0] = mode; sc[1] = cur_cut; sc[2] = cur_mp; sc[3] = nmoves;
+            }
+        }
+        ++steps;
+        __syncthreads();
+    }
+    __syncthreads();
+    // the kept state
+    for (int64_t v = threadIdx.x; v < n; v += CT) R.part[v] = R.best[v];
+    for (int q = threadIdx.x; q < k; q += CT) R.pw[q] = s_best[q];
+    if (threadIdx.x == 0) R.out[0] = steps;
+}
+
+static size_t cta_refine_smem(int32_t k) {
+    const size_t head = (((size_t)(4 * k + 1) * 8 + k + 15) & ~(size_t)15);
+    const size_t hist = sizeof(int32_t) * CW * (size_t)k, keys = sizeof(uint64_t) * kCtaMaxN;
+    return head + (hist > keys ? hist : keys);
+}
+
+void refine_smem_caps() {
+    GP_CUDA(cudaFuncSetAttribute(k_refine_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_refine_smem(GP_MAX_K)));
+    GP_CUDA(cudaFuncSetAttribute(k_rb_step_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_refine_smem(GP_MAX_K)));
+}
+
+static bool cta_refine_ok(const Level& L, const Params& P) {
+    const int64_t lim = std::min<int64_t>(P.o.small_level_n, kCtaMaxN);
+    return P.o.small_level_n > 0 && L.nheavy == 0 && L.g.n <= lim && P.k <= GP_MAX_K;
+}
+
+static int refine_level_cta(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr) {
+    const DGraph& g = L.g;
+    const int64_t n = g.n;
+    auto mk = c.tmp->save();
+    CtaRefineArgs R;
+    R.g = g; R.k = P.k; R.Lmax = P.Lmax; R.den = P.o.lp_filter_den; R.max_iters = P.o.refine_max_iters;
+    R.patience = P.o.refine_patience; R.strong_after = P.o.strong_after;
+    for (int b = 0; b < 3; ++b) { R.bucket[b] = L.bucket[b]; R.nbucket[b] = L.nbucket[b]; R.clist[b] = B.clist[b]; }
+    R.part = B.part; R.part_next = B.part_next; R.lock = B.lock; R.lock_next = B.lock_next; R.best = B.best;
+    R.pw = B.pw; R.dest = B.dest; R.gain = B.gain; R.status = B.status;
+    R.pre = c.tmp_alloc<int64_t>(n);
+    R.flag = c.tmp_alloc<int32_t>(n);
+    R.gkeys = c.tmp_alloc<uint64_t>(n);
+    R.tr_arrays = nullptr; R.tr_scalars = nullptr;
+    if (tr.on()) {
+        R.tr_arrays = c.tmp_alloc<int32_t>((int64_t)P.o.refine_max_iters * 3 * n);
+        R.tr_scalars = c.tmp_alloc<int64_t>((int64_t)P.o.refine_max_iters * 4);
+    }
+    R.out = c.tmp_alloc<int64_t>(1);
+    k_refine_cta<<<1, CT, cta_refine_smem(P.k), c.s>>>(R);
+    GP_LAUNCHED(c);
+    const int steps = (int)read_i64(c, R.out);
+    // each step: one connectivity pass plus its move step; one closing pass
+    c.bytes += (int64_t)(steps + 1) * (L.scan_bytes() + 13 * n) + (int64_t)steps * (9 * n + 16 * n);
+    if (tr.on() && steps > 0) {
+        std::vector<int32_t> arr((size_t)steps * 3 * n);
+        std::vector<int64_t> sc((size_t)steps * 4);
+        GP_CUDA(cudaMemcpyAsync(arr.data(), R.tr_arrays, sizeof(int32_t) * arr.size(), cudaMemcpyDeviceToHost, c.s));
+        GP_CUDA(cudaMemcpyAsync(sc.data(), R.tr_scalars, sizeof(int64_t) * sc.size(), cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        for (int it = 0; it < steps; ++it) {
+            gp_trace_event ev;
+            memset(&ev, 0, sizeof ev);
+            ev.kind = GP_TR_REFINE_ITER; ev.level = level; ev.iter = it; ev.mode = (int32_t)sc[4 * it];
+            ev.n = n; ev.m = g.m; ev.cut = sc[4 * it + 1]; ev.maxpw = sc[4 * it + 2]; ev.count = sc[4 * it + 3];
+            int32_t* base = arr.data() + (size_t)it * 3 * n;
+            ev.a0 = base; ev.a1 = base + n; ev.a2 = base + 2 * n;
+            tr.emit(ev);
+        }
+    }
+    c.tmp->restore(mk);
+    return steps;
+}
+
 // ------------------------------------------------------------------ level controller
 static int bits_for(int64_t x) {
     int b = 1;
@@ -774,6 +1222,7 @@ static void trace_iter(Ctx& c, const RefineBufs& B, int64_t n, int64_t m, int le
 }
 
 int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr) {
+    if (cta_refine_ok(L, P)) return refine_level_cta(c, L, P, B, level, tr);
     const DGraph& g = L.g;
     const int64_t n = g.n;
     const int32_t k = P.k;
@@ -869,6 +1318,17 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             c.bytes += 9 * n + 16 * nlist + cdeg * (4 + (g.ew ? 4 : 0) + 12);
             std::swap(B.part, B.part_next);
             std::swap(B.lock, B.lock_next);
+        } else if (n <= kCtaMaxN) {
+            // the whole step in one thread block
+            auto mk = c.tmp->save();
+            RbCta RA;
+            RA.vw = g.vw; RA.part = B.part; RA.lock = B.lock; RA.dest = B.dest; RA.gain = B.gain;
+            RA.pre = c.tmp_alloc<int64_t>(n); RA.flag = c.tmp_alloc<int32_t>(n); RA.gkeys = c.tmp_alloc<uint64_t>(n);
+            RA.k = k; RA.Lmax = Lmax;
+            k_rb_step_cta<<<1, CT, cta_refine_smem(k), c.s>>>(RA, mode, n, nullptr, 0, B.pw, moves_d);
+            GP_LAUNCHED(c);
+            c.bytes += 4 * n + 12 * n + 80 * n;
+            c.tmp->restore(mk);
         } else {
             memset_async(c, B.lock, 0, n);
             auto mk = c.tmp->save();
@@ -880,7 +1340,18 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             scan_excl_i32_to_i64(c, flag, vpos, n, vpos + n);
             const int64_t ncand = read_i64(c, vpos + n);
             c.bytes += 4 * n + 12 * n;
-            if (ncand > 0) {
+            if (ncand > 0 && ncand <= kCtaMaxN) {
+                // few candidates: sort, select and apply in one thread block
+                k_rb_compact<<<grid_for(n, 256), 256, 0, c.s>>>(n, flag, vpos, B.part, B.gain, B.ckeys, B.cvals);
+                GP_LAUNCHED(c);
+                RbCta RA;
+                RA.vw = g.vw; RA.part = B.part; RA.lock = B.lock; RA.dest = B.dest; RA.gain = B.gain;
+                RA.pre = c.tmp_alloc<int64_t>(ncand); RA.flag = c.tmp_alloc<int32_t>(ncand);
+                RA.gkeys = c.tmp_alloc<uint64_t>(ncand); RA.k = k; RA.Lmax = Lmax;
+                k_rb_step_cta<<<1, CT, cta_refine_smem(k), c.s>>>(RA, mode, n, B.cvals, ncand, B.pw, moves_d);
+                GP_LAUNCHED(c);
+                c.bytes += 80 * ncand;
+            } else if (ncand > 0) {
                 k_rb_compact<<<grid_for(n, 256), 256, 0, c.s>>>(n, flag, vpos, B.part, B.gain, B.ckeys, B.cvals);
                 GP_LAUNCHED(c);
                 const int bits = RB_SHIFT + nb_k;
