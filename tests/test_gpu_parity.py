@@ -27,6 +27,8 @@ def _cases():
     # a hub of 40000 leaves: rows split over several CTAs, longest contraction tier
     yield "megahub_k8", star_plus_grid(leaves=40000, side=64), 8, 0.03, None, {}
     yield "megahub_w_k3", star_plus_grid(leaves=36000, side=40), 3, 0.05, "w", {"coarsen_to": 300}
+    # a 150000-leaf hub: its coarse row is contracted by several CTAs sharing one table
+    yield "gigahub_k4", star_plus_grid(leaves=150000, side=32), 4, 0.03, None, {}
     yield "rmat11_k64_tight", graphs.rmat(11, seed=3)[:2], 64, 0.0, None, {}
     yield "er_k3_nohop", graphs.erdos_renyi(3000, 3.0, seed=5), 3, 0.02, None, {"two_hop": -1}
     yield "rgg_k2", graphs.random_geometric(4000, 8.0, seed=6), 2, 0.03, None, {"init_trials": 8}

@@ -189,6 +189,7 @@ struct MatchArgs {
     int64_t* nkeys;
     int nbits;
     const int32_t* prio;      // learned priorities per entry (nullptr: edge weights)
+    const uint8_t* hdead;     // MODE 0: heavy rows left without an eligible neighbour (nullptr: none)
 };
 
 // high word of an entry's matching priority: learned score or edge weight
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
         // the partial bests of all its pieces in item order
         const int32_t h = A.item_row[blockIdx.x];
         const int64_t v = A.heavy[h];
-        if (A.match[v] != -1) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
+        if (A.match[v] != -1 || (A.hdead && A.hdead[h])) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
         const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
         uint64_t bk = 0; int32_t bid = -1;
         const int64_t end = A.item_end[blockIdx.x];
@@ -344,11 +345,15 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
 
 // Mutual proposals become pairs; vertices left unmatched go to the next
 // round's worklists, bucketed by degree (any order: each vertex's proposal is
-// its own).  Heavy vertices are not listed: their CTAs check match[] directly.
+// its own).  A vertex that proposed nobody has no unmatched neighbour within
+// the weight cap, and never will (vertices only become matched), so it leaves
+// the worklists; a heavy one is flagged in hdead instead (heavy vertices are
+// not listed: their CTAs check match[] and hdead[] directly).  next_n[3]
+// counts the heavy vertices still live.
 __global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, const int32_t* l1, const int32_t* l2,
                             int64_t n0, int64_t n1, int64_t n2, const int32_t* __restrict__ heavy, int64_t nheavy,
                             const int32_t* __restrict__ prop, int32_t* __restrict__ match, int64_t* __restrict__ pairs,
-                            int32_t* nl0, int32_t* nl1, int32_t* nl2, int64_t* next_n) {
+                            int32_t* nl0, int32_t* nl1, int32_t* nl2, int64_t* next_n, uint8_t* __restrict__ hdead) {
     int64_t local = 0;
     const int64_t total = n0 + n1 + n2 + nheavy;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -359,13 +364,18 @@ __global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, c
         else if (i < n0 + n1) v = l1[i - n0];
         else if (i < n0 + n1 + n2) v = l2[i - n0 - n1];
         else if (i < total) v = heavy[i - n0 - n1 - n2];
+        const bool is_heavy = i >= n0 + n1 + n2;
         bool left = false;
         int64_t d = 0;
-        if (v >= 0 && match[v] == -1) {
+        if (v >= 0 && match[v] == -1 && !(is_heavy && hdead[i - n0 - n1 - n2])) {
             const int32_t u = prop[v];
             if (u >= 0 && prop[u] == (int32_t)v) {
                 match[v] = u;
                 if (v < u) ++local;
+            } else if (u < 0) {
+                if (is_heavy) hdead[i - n0 - n1 - n2] = 1;
+            } else if (is_heavy) {
+                atomicAdd((unsigned long long*)&next_n[3], 1ull);
             } else {
                 left = true;
                 d = rp[v + 1] - rp[v];
@@ -427,27 +437,32 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     A.hdone = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nheavy, 1));
     memset_async(c, A.hdone, 0, sizeof(int32_t) * std::max<int64_t>(L.nheavy, 1));
     A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0; A.prio = prio;
+    uint8_t* hdead = c.tmp_alloc<uint8_t>(std::max<int64_t>(L.nheavy, 1));
+    memset_async(c, hdead, 0, std::max<int64_t>(L.nheavy, 1));
+    A.hdead = hdead;
     for (int b = 0; b < 3; ++b) { A.list[b] = L.bucket[b]; A.nlist[b] = L.nbucket[b]; }
-    int64_t pairs = 0;
+    int64_t pairs = 0, heavy_live = L.nheavy;
     int rounds = 0;
     for (int r = 0; r < P.o.match_rounds; ++r) {
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
-        if (units == 0 && L.nheavy == 0) break;
+        // nobody left who can propose: this round would add no pair
+        if (units == 0 && heavy_live == 0) { rounds = r + 1; break; }
         const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * 8);
-        memset_async(c, d_cnt, 0, 4 * sizeof(int64_t));
+        memset_async(c, d_cnt, 0, 5 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);
         int32_t** nxt = wl[r & 1];
         const int64_t tot = A.nlist[0] + A.nlist[1] + A.nlist[2] + L.nheavy;
         k_handshake<<<grid_for(tot, 256), 256, 0, c.s>>>(g.rp, A.list[0], A.list[1], A.list[2], A.nlist[0], A.nlist[1],
                                                          A.nlist[2], L.heavy, L.nheavy, prop, match, d_cnt, nxt[0],
-                                                         nxt[1], nxt[2], d_cnt + 1);
+                                                         nxt[1], nxt[2], d_cnt + 1, hdead);
         GP_LAUNCHED(c);
         const int64_t share = g.n ? (tot * 1000) / g.n : 0;
         c.bytes += (L.scan_bytes() + 4 * g.m) * share / 1000 + 16 * tot;
-        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_cnt, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+        GP_CUDA(cudaMemcpyAsync(c.h_pinned, d_cnt, 5 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
         c.sync();
         const int64_t newp = c.h_pinned[0];
+        heavy_live = c.h_pinned[4];
         rounds = r + 1;
         pairs += newp;
         for (int b = 0; b < 3; ++b) { A.list[b] = nxt[b]; A.nlist[b] = c.h_pinned[1 + b]; }
@@ -461,6 +476,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         int32_t* vals2 = c.tmp_alloc<int32_t>(g.n);
         memset_async(c, d_cnt, 0, 2 * sizeof(int64_t));
         MatchArgs B2 = A;
+        B2.hdead = nullptr;   // anchors: the top neighbour over all neighbours
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
         const int64_t units = (B2.nlist[0] + 3) / 4 + B2.nlist[1] + B2.nlist[2];
@@ -804,26 +820,136 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
     }
 }
 
-// tier D: each CTA owns a table region of region_slots slots (sized for the
-// longest row) and reuses it row after row; few CTAs keep the working set in L2
-__global__ void __launch_bounds__(TD_T) k_dedup_cta_global(const int32_t* __restrict__ list, int64_t nlist,
-                                                           const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                           int64_t region_slots, int64_t region_ints,
-                                                           int32_t* __restrict__ gtab,
-                                                           const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
-                                                           int32_t* __restrict__ tci, int32_t* __restrict__ tew,
-                                                           int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
-    __shared__ int32_t sh[33];
-    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
-        const int64_t c = list[li];
-        const int64_t deg = cdeg[c];
-        int64_t S = 1;
-        int lg = 0;
-        while (S < 2 * deg) { S <<= 1; ++lg; }
-        int32_t* keys = gtab + region_ints * (int64_t)blockIdx.x;
-        cta_dedup<TD_T>(mapped, mw, off[c], deg, (int32_t)c, keys, keys + S, keys + 2 * S, S, lg, keys + 3 * region_slots,
-                        tci, tew, &cnt[c], sh, err);
+// tier D split over CTAs: rows longer than TC_ROW are cut into pieces of
+// TD_PIECE entries, one CTA each, all pieces of a row sharing that row's
+// global table.  D1 inserts (first position kept as the largest deg - j by
+// atomicMax, so that a zero-filled table starts empty), D2 ballots the
+// first-occurrence flags of each 32-entry word, a device-wide scan of the word
+// popcounts ranks the words of every row, D3 writes the first occurrences at
+// their ranks.  Same output as one CTA per row: unique neighbours in order of
+// first occurrence with summed weights.
+constexpr int64_t TD_PIECE = 65536;   // multiple of 32
+struct TierD {
+    const int32_t* rc;      // coarse row of each tier-D row
+    const int32_t* rlg;     // log2 of its table size
+    const int64_t* rtab;    // table offset
+    const int64_t* rword;   // first word of the row in the word arrays
+    const int32_t* prow;    // row of each piece
+    const int64_t* pbeg;    // entry range of the piece within the row
+    const int64_t* pend;
+    int32_t* keys;          // tables: keys (filled with EMPTY_KEY), first position, weight sum
+    int32_t* pos;
+    int32_t* wsum;
+    uint32_t* bits;         // first-occurrence flags, one word per 32 entries
+    int32_t* wcnt;          // their popcounts
+    const int64_t* wpre;    // exclusive prefix of wcnt (+ total)
+};
+
+__device__ __forceinline__ uint32_t td_lookup(const int32_t* keys, int32_t cu, int lg) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t h = slot_hash(cu, lg);
+    for (uint32_t probe = 0; probe <= mask && keys[h] != cu; ++probe) h = (h + 1) & mask;
+    return h;
+}
+
+__global__ void __launch_bounds__(TD_T) k_td_insert(TierD D, const int64_t* __restrict__ off,
+                                                    const int64_t* __restrict__ cdeg,
+                                                    const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
+                                                    int32_t* __restrict__ err) {
+    const int32_t r = D.prow[blockIdx.x];
+    const int32_t self = D.rc[r];
+    const int lg = D.rlg[r];
+    const uint32_t mask = (1u << lg) - 1u;
+    int32_t* keys = D.keys + D.rtab[r];
+    int32_t* pos = D.pos + D.rtab[r];
+    int32_t* wsum = D.wsum + D.rtab[r];
+    const int64_t o = off[self], deg = cdeg[self], end = D.pend[blockIdx.x];
+    for (int64_t base = D.pbeg[blockIdx.x]; base < end; base += 4 * TD_T) {
+        int32_t cu[4], wt[4], old[4];
+        uint32_t h[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int64_t j = base + c * TD_T + threadIdx.x;
+            cu[c] = j < end ? __ldcs(&mapped[o + j]) : self;
+            wt[c] = j < end ? __ldcs(&mw[o + j]) : 0;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            h[c] = slot_hash(cu[c], lg);
+            old[c] = cu[c] != self ? atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]) : EMPTY_KEY;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (cu[c] == self) continue;
+            uint32_t probe = 1;
+            while (old[c] != EMPTY_KEY && old[c] != cu[c] && probe <= mask) {
+                h[c] = (h[c] + 1) & mask;
+                old[c] = atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]);
+                ++probe;
+            }
+            if (old[c] != EMPTY_KEY && old[c] != cu[c]) { atomicExch(err, 1); continue; }
+            const int64_t j = base + c * TD_T + threadIdx.x;
+            atomicMax(&pos[h[c]], (int32_t)(deg - j));
+            atomicAdd(&wsum[h[c]], wt[c]);
+        }
     }
+}
+
+__global__ void __launch_bounds__(TD_T) k_td_flags(TierD D, const int64_t* __restrict__ off,
+                                                   const int64_t* __restrict__ cdeg,
+                                                   const int32_t* __restrict__ mapped) {
+    const int32_t r = D.prow[blockIdx.x];
+    const int32_t self = D.rc[r];
+    const int lg = D.rlg[r];
+    const int32_t* keys = D.keys + D.rtab[r];
+    const int32_t* pos = D.pos + D.rtab[r];
+    const int64_t o = off[self], deg = cdeg[self];
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = D.pbeg[blockIdx.x] / 32, w1 = (D.pend[blockIdx.x] + 31) / 32;
+    for (int64_t wi = w0 + (threadIdx.x >> 5); wi < w1; wi += TD_T / 32) {
+        const int64_t j = wi * 32 + lane;
+        bool first = false;
+        if (j < deg) {
+            const int32_t cu = mapped[o + j];
+            if (cu != self) first = pos[td_lookup(keys, cu, lg)] == (int32_t)(deg - j);
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, first);
+        if (lane == 0) {
+            D.bits[D.rword[r] + wi] = word;
+            D.wcnt[D.rword[r] + wi] = __popc(word);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TD_T) k_td_write(TierD D, const int64_t* __restrict__ off,
+                                                   const int64_t* __restrict__ cdeg,
+                                                   const int32_t* __restrict__ mapped, int32_t* __restrict__ tci,
+                                                   int32_t* __restrict__ tew, int32_t* __restrict__ rowcnt) {
+    const int32_t r = D.prow[blockIdx.x];
+    const int32_t self = D.rc[r];
+    const int lg = D.rlg[r];
+    const int32_t* keys = D.keys + D.rtab[r];
+    const int32_t* wsum = D.wsum + D.rtab[r];
+    const int64_t o = off[self], deg = cdeg[self];
+    const int64_t rw = D.rword[r], nwords = (deg + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int64_t w0 = D.pbeg[blockIdx.x] / 32, w1 = (D.pend[blockIdx.x] + 31) / 32;
+    for (int64_t wi = w0 + (threadIdx.x >> 5); wi < w1; wi += TD_T / 32) {
+        const uint32_t word = D.bits[rw + wi];
+        if (!((word >> lane) & 1u)) continue;
+        const int32_t cu = mapped[o + wi * 32 + lane];
+        const int64_t rank = D.wpre[rw + wi] - D.wpre[rw] + __popc(word & lt);
+        tci[o + rank] = cu;
+        tew[o + rank] = wsum[td_lookup(keys, cu, lg)];
+    }
+    if (D.pbeg[blockIdx.x] == 0 && threadIdx.x == 0) rowcnt[self] = (int32_t)(D.wpre[rw + nwords] - D.wpre[rw]);
+}
+
+__global__ void k_td_rows(const int32_t* __restrict__ list, int64_t n, const int64_t* __restrict__ cdeg,
+                          int64_t* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = cdeg[list[i]];
 }
 
 // warp per coarse row: temporary (walk-bound offsets) -> final CSR
@@ -899,13 +1025,65 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         GP_LAUNCHED(c);
     }
     if (nD > 0) {
-        int64_t S = 1;
-        while (S < 2 * maxD) S <<= 1;
-        const int64_t ctas = std::min<int64_t>(nD, 96);
-        const int64_t region_ints = 3 * S + 2 * ((maxD + 31) / 32);
-        int32_t* gtab = c.tmp_alloc<int32_t>(region_ints * ctas);
-        k_dedup_cta_global<<<(unsigned)ctas, TD_T, 0, c.s>>>(listD, nD, off, cdeg, S, region_ints, gtab, mapped, mw,
-                                                             tci, tew, rowcnt, err);
+        (void)maxD;
+        // row lengths to the host: tables, word ranges and pieces
+        int64_t* d_deg = c.tmp_alloc<int64_t>(nD);
+        k_td_rows<<<grid_for(nD, 256), 256, 0, c.s>>>(listD, nD, cdeg, d_deg);
+        GP_LAUNCHED(c);
+        std::vector<int64_t> hdeg((size_t)nD);
+        std::vector<int32_t> hlist((size_t)nD);
+        GP_CUDA(cudaMemcpyAsync(hdeg.data(), d_deg, sizeof(int64_t) * nD, cudaMemcpyDeviceToHost, c.s));
+        GP_CUDA(cudaMemcpyAsync(hlist.data(), listD, sizeof(int32_t) * nD, cudaMemcpyDeviceToHost, c.s));
+        c.sync();
+        std::vector<int32_t> rlg((size_t)nD), prow;
+        std::vector<int64_t> rtab((size_t)nD), rword((size_t)nD), pbeg, pend;
+        int64_t tab = 0, words = 0;
+        for (int64_t r = 0; r < nD; ++r) {
+            int64_t S = 2;
+            int lg = 1;
+            while (S < 2 * hdeg[r]) { S <<= 1; ++lg; }
+            rlg[r] = lg; rtab[r] = tab; rword[r] = words;
+            tab += S;
+            words += (hdeg[r] + 31) / 32;
+            for (int64_t b = 0; b < hdeg[r]; b += TD_PIECE) {
+                prow.push_back((int32_t)r);
+                pbeg.push_back(b);
+                pend.push_back(std::min<int64_t>(b + TD_PIECE, hdeg[r]));
+            }
+        }
+        const int64_t np = (int64_t)prow.size();
+        TierD D;
+        int32_t* d_rc = c.tmp_alloc<int32_t>(nD);
+        int32_t* d_rlg = c.tmp_alloc<int32_t>(nD);
+        int64_t* d_rtab = c.tmp_alloc<int64_t>(nD);
+        int64_t* d_rword = c.tmp_alloc<int64_t>(nD);
+        int32_t* d_prow = c.tmp_alloc<int32_t>(np);
+        int64_t* d_pbeg = c.tmp_alloc<int64_t>(np);
+        int64_t* d_pend = c.tmp_alloc<int64_t>(np);
+        GP_CUDA(cudaMemcpyAsync(d_rc, hlist.data(), sizeof(int32_t) * nD, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_rlg, rlg.data(), sizeof(int32_t) * nD, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_rtab, rtab.data(), sizeof(int64_t) * nD, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_rword, rword.data(), sizeof(int64_t) * nD, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_prow, prow.data(), sizeof(int32_t) * np, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_pbeg, pbeg.data(), sizeof(int64_t) * np, cudaMemcpyHostToDevice, c.s));
+        GP_CUDA(cudaMemcpyAsync(d_pend, pend.data(), sizeof(int64_t) * np, cudaMemcpyHostToDevice, c.s));
+        D.rc = d_rc; D.rlg = d_rlg; D.rtab = d_rtab; D.rword = d_rword;
+        D.prow = d_prow; D.pbeg = d_pbeg; D.pend = d_pend;
+        D.keys = c.tmp_alloc<int32_t>(tab);
+        D.pos = c.tmp_alloc<int32_t>(2 * tab);
+        D.wsum = D.pos + tab;
+        D.bits = (uint32_t*)c.tmp_alloc<int32_t>(words);
+        D.wcnt = c.tmp_alloc<int32_t>(words);
+        int64_t* wpre = c.tmp_alloc<int64_t>(words + 1);
+        D.wpre = wpre;
+        GP_CUDA(cudaMemsetAsync(D.keys, 0xff, sizeof(int32_t) * tab, c.s));
+        GP_CUDA(cudaMemsetAsync(D.pos, 0, sizeof(int32_t) * 2 * tab, c.s));
+        k_td_insert<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped, mw, err);
+        GP_LAUNCHED(c);
+        k_td_flags<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped);
+        GP_LAUNCHED(c);
+        scan_excl_i32_to_i64(c, D.wcnt, wpre, words, wpre + words);
+        k_td_write<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
     int64_t* crp = c.keep_alloc<int64_t>(nc + 1);
