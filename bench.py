@@ -58,6 +58,8 @@ def parse_args():
                     help="rmat: one R-MAT graph (default); batch: the batched configuration")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick workers / launch-shape options on a sample first (untimed; results are identical)")
     ap.add_argument("--profile-once", action="store_true",
                     help="one warm partition, then exactly one partition between cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off); prints nothing else")
@@ -226,6 +228,14 @@ def run_batch(args, rank, world, dev, dist):
     m_local = sum(g[1].numel() // 2 for g in gs)
     n_local = sum(g[0].numel() - 1 for g in gs)
     opts = make_options()
+    tuned = None
+    if args.autotune:
+        from thegraphpartitioning_b200.autotune import autotune_batch
+        best = autotune_batch(gs, ks, args.imbalance, seeds, sample=min(256, len(gs)))
+        opts, args.workers = best["options"], best["workers"]
+        tuned = {"sample_graphs": best["sample"], "workers": best["workers"],
+                 "small_level_n": int(opts.small_level_n), "ctas_per_sm": int(opts.ctas_per_sm),
+                 "candidates": len(best["table"])}
     stream = torch.cuda.current_stream(dev)
     outs = [torch.empty(g[0].numel() - 1, dtype=torch.int32, device=dev) for g in gs]
     for _ in range(args.warmup):
@@ -281,7 +291,8 @@ def run_batch(args, rank, world, dev, dist):
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RGG + Erdos-Renyi batch)",
             "config": {"workload": f"batch{args.batch_count}_rgg_er", "graphs": args.batch_count,
                        "vertices": n_all, "m_undirected": m_all, "ks": "2,4,8,16,32", "imbalance": args.imbalance,
-                       "workers_per_gpu": args.workers, "parallelism": f"graph shards x{world} (LPT)"},
+                       "workers_per_gpu": args.workers, "parallelism": f"graph shards x{world} (LPT)",
+                       "autotune": tuned},
             "result": {"sum_of_cuts": int(cut_sum)},
             "roofline": {"bound": "hbm", "kernel": "k_conn (refinement connectivity pass)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,

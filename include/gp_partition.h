@@ -72,7 +72,11 @@ typedef struct gp_options {
                                    one thread block, one launch per level; 0 or < 0:
                                    off.  Results are identical either way; it pays
                                    only where launches, not SMs, are scarce            */
-    int32_t reserved[3];
+    int32_t ctas_per_sm;        /* grid of the neighbour-scan kernels (matching rounds,
+                                   connectivity pass, afterburner): this many 256-thread
+                                   CTAs per SM at most (0: 8); results are identical for
+                                   every value (tuning knob of the autotuner)          */
+    int32_t reserved[2];
 } gp_options;
 
 /* Result record of one call. */

@@ -44,3 +44,23 @@ def test_batch_reports_invalid_graph(gp, cuda):
     with pytest.raises(gp.GPError) as ei:
         gp.partition_batch(gs, [2, 2])
     assert ei.value.code == -1
+
+
+def test_autotune_picks_a_config_with_identical_results(gp, cuda):
+    """The autotuner times launch-shape candidates on a sample; whatever it
+    picks, every partition equals the default call's."""
+    from thegraphpartitioning_b200.autotune import autotune_batch, autotune_graph
+    specs, gs = _batch(cuda, count=12, seed=3)
+    ks = [s["k"] for s in specs]
+    seeds = [s["seed"] for s in specs]
+    best = autotune_batch(gs, ks, 0.03, seeds, sample=6, workers=(1, 4), small_level_n=(0, 2048),
+                          ctas_per_sm=(2, 8))
+    assert len(best["table"]) == 8 and best["sample"] == 6
+    ref, _ = gp.partition_batch(gs, ks, 0.03, seeds)
+    got, _ = gp.partition_batch(gs, ks, 0.03, seeds, options=best["options"], workers=best["workers"])
+    assert all(torch.equal(x, y) for x, y in zip(ref, got))
+    rp, ci = gs[0]
+    one = autotune_graph(rp, ci, ks[0], seed=seeds[0], ctas_per_sm=(2, 16), small_level_n=(0, 4096))
+    assert len(one["table"]) == 4
+    p1, _, _ = gp.partition(rp, ci, ks[0], 0.03, seeds[0], options=one["options"])
+    assert torch.equal(p1, ref[0])

@@ -39,6 +39,7 @@ def _cases():
     yield "weighted_k5_mixed", graphs.grid2d(40, 50), 5, 0.05, "w", {"small_level_n": 1200}
     yield "chunglu_k8_mixed", graphs.chung_lu(12000, 40000, seed=2), 8, 0.03, None, {"small_level_n": 3000}
     yield "er_k64_cta", graphs.erdos_renyi(16000, 8.0, seed=8), 64, 0.03, None, {"small_level_n": 16384}
+    yield "rmat12_k16_ctas2", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"ctas_per_sm": 2}
     # exact balance on 50k-60k vertices: rebalance steps with more candidates
     # than one thread block sorts (radix-sorted multi-kernel path), weak and strong
     yield "rgg50k_k2_bigrb", graphs.random_geometric(50000, 8.0, seed=9), 2, 0.0, None, {}

@@ -49,7 +49,8 @@ class GpOptions(C.Structure):
         ("verbose", C.c_int32),
         ("profile", C.c_int32),
         ("small_level_n", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("ctas_per_sm", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

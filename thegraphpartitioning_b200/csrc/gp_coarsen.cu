@@ -447,7 +447,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
         // nobody left who can propose: this round would add no pair
         if (units == 0 && heavy_live == 0) { rounds = r + 1; break; }
-        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * 8);
+        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * P.o.ctas_per_sm);
         memset_async(c, d_cnt, 0, 5 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);

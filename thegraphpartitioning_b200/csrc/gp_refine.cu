@@ -1231,7 +1231,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const int kpad = (k + 15) & ~15;
     const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
     // at most 1024 + 32 * GP_MAX_K bytes: below the 48 KB default, no attribute needed
-    const int light_blocks = grid_for(n * 32, RT, c.sm_count * 8);
+    const int light_blocks = grid_for(n * 32, RT, c.sm_count * P.o.ctas_per_sm);
     const int grid = (int)L.nitems + light_blocks;
     int64_t best_cut = 0, best_mp = 0;
     int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
