@@ -206,6 +206,9 @@ int gp_gnn_get_params(const gp_gnn* model, float* params, int32_t nparams);
  * hash tie-break */
 int gp_gnn_set_prio_bits(gp_gnn* model, int32_t bits);
 int gp_gnn_get_prio_bits(const gp_gnn* model);
+/* learned priorities at levels 0..level only, edge weights above (-1: every level) */
+int gp_gnn_set_max_level(gp_gnn* model, int32_t level);
+int gp_gnn_get_max_level(const gp_gnn* model);
 /* per-entry priorities (int32, may be NULL) and logits (float, may be NULL) of one graph */
 int gp_gnn_forward_device(gp_gnn* model, int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
                           const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t level, void* stream,

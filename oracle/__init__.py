@@ -80,8 +80,8 @@ def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
     """Full V-cycle on the CPU.  Returns (part, stats_dict, events).
 
     prio_levels: {level: int32[m_level]} matching priorities replacing the edge
-    weights (the learned mode); the oracle asks for every level it coarsens and
-    fails when a level or its entry count is missing."""
+    weights (the learned mode) at the levels listed; other levels use the edge
+    weights.  Fails when a listed level's entry count differs."""
     lib = _load()
     rp = _as(rowptr, np.int64)
     ci = _as(colidx, np.int32)
@@ -102,7 +102,9 @@ def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
 
         def cb(_user, level, m):
             a = held.get(int(level))
-            if a is None or len(a) != int(m):
+            if a is None:
+                return None
+            if len(a) != int(m):
                 missing.append((int(level), int(m)))
                 return None
             return a.ctypes.data
@@ -112,7 +114,7 @@ def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
                                     int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st), tfn, None,
                                     C.cast(pfn, C.c_void_p), None)
         if missing:
-            raise OracleError(-1, f"no priorities for (level, m) = {missing}")
+            raise OracleError(-1, f"priorities of the wrong length for (level, m) = {missing}")
     if rc != 0:
         raise OracleError(rc, lib.gpo_last_error().decode())
     return part[:n], st.as_dict(), (col.events if col else [])

@@ -102,17 +102,20 @@ def test_learned_vcycle_matches_oracle(oracle_mod, gp, cuda):
     """The integer path of the learned mode is the plain path with the
     priorities substituted: the oracle, given the GPU's per-level priorities,
     reproduces every event of the learned run."""
-    for g, k, w, seed in ((graphs.rmat(13, seed=21)[:2], 16, False, 3),
-                          (graphs.grid2d(70, 60), 6, True, 4)):
+    for g, k, w, seed, max_level in ((graphs.rmat(13, seed=21)[:2], 16, False, 3, -1),
+                                     (graphs.grid2d(70, 60), 6, True, 4, -1),
+                                     (graphs.rmat(13, seed=22)[:2], 8, False, 5, 0)):
         rp, ci = to_np(*g)
         ew = vw = None
         if w:
             ew, vw = weighted(rp, ci, seed=7)
-        model = gp.GNN(_params(3))
+        model = gp.GNN(_params(3), prio_bits=10, max_level=max_level)
         part, st, rep, ev = gp.partition_learned(_dev(rp, cuda), _dev(ci, cuda), k, model, 0.03, seed,
                                                  vwgt=_dev(vw, cuda), ewgt=_dev(ew, cuda), judge=False, trace=True)
         prio = {e["level"]: e["a0"] for e in ev if e["kind"] == GP_TR_PRIO}
         assert prio and rep["kept_learned"] == 1
+        if max_level >= 0:
+            assert set(prio) == set(range(max_level + 1))
         ev_gpu = [e for e in ev if e["kind"] != GP_TR_PRIO]
         p_ref, s_ref, ev_ref = oracle_mod.partition(rp, ci, k, 0.03, seed, vwgt=vw, ewgt=ew, trace=True,
                                                     prio_levels=prio)

@@ -80,6 +80,10 @@ def lib():
     L.gp_gnn_set_prio_bits.argtypes = [VP, C.c_int32]
     L.gp_gnn_get_prio_bits.restype = C.c_int
     L.gp_gnn_get_prio_bits.argtypes = [VP]
+    L.gp_gnn_set_max_level.restype = C.c_int
+    L.gp_gnn_set_max_level.argtypes = [VP, C.c_int32]
+    L.gp_gnn_get_max_level.restype = C.c_int
+    L.gp_gnn_get_max_level.argtypes = [VP]
     L.gp_gnn_get_params.restype = C.c_int
     L.gp_gnn_get_params.argtypes = [VP, C.POINTER(C.c_float), C.c_int32]
     L.gp_gnn_forward_device.restype = C.c_int
@@ -247,12 +251,22 @@ class GNN:
     gp_partition_learned_device.  Parameters are a flat float32 array of
     num_params() values in the layout oracle/gnn_ref.py documents."""
 
-    def __init__(self, params=None, prio_bits: int = 16):
+    def __init__(self, params=None, prio_bits: int = 16, max_level: int = -1):
         self._h = C.c_void_p()
         _check(lib().gp_gnn_create(C.byref(self._h)))
         if params is not None:
             self.set_params(params)
         self.prio_bits = prio_bits
+        self.max_level = max_level
+
+    @property
+    def max_level(self) -> int:
+        """Learned priorities at levels 0..max_level, edge weights above (-1: all)."""
+        return int(lib().gp_gnn_get_max_level(self._h))
+
+    @max_level.setter
+    def max_level(self, level: int) -> None:
+        _check(lib().gp_gnn_set_max_level(self._h, int(level)))
 
     @property
     def prio_bits(self) -> int:
@@ -277,16 +291,17 @@ class GNN:
         return p
 
     def save(self, path: str) -> None:
-        """params (float32) and prio_bits in one .npz file."""
+        """params (float32), prio_bits and max_level in one .npz file."""
         with open(path, "wb") as f:
-            np.savez(f, params=self.get_params(), prio_bits=np.int32(self.prio_bits))
+            np.savez(f, params=self.get_params(), prio_bits=np.int32(self.prio_bits),
+                     max_level=np.int32(self.max_level))
 
     @classmethod
     def load(cls, path: str) -> "GNN":
         z = np.load(path)
         if isinstance(z, np.ndarray):        # bare parameter array
             return cls(z)
-        return cls(z["params"], int(z["prio_bits"]))
+        return cls(z["params"], int(z["prio_bits"]), int(z["max_level"]) if "max_level" in z.files else -1)
 
     def forward(self, rowptr, colidx, vwgt=None, ewgt=None, level: int = 0, stream=None):
         """(priority int32[m], logit float32[m]) CUDA tensors of one graph."""

@@ -250,7 +250,8 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
             auto mk = c.tmp->save();
             int32_t* match = c.tmp_alloc<int32_t>(lv.back().g.n);
             int32_t* prio = nullptr;
-            if (P.gnn) {
+            const bool scored = P.gnn && gnn_scores_level(P.gnn, level);
+            if (scored) {
                 prio = c.tmp_alloc<int32_t>(lv.back().g.m);
                 GP_CUDA(cudaEventRecord(tm.e[4], c.s));
                 gnn_level_priorities(c, P.gnn, lv.back(), level, prio);
@@ -265,7 +266,7 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
             }
             int rounds = 0;
             const int64_t pairs = match_level(c, lv.back(), level, P, match, &rounds, prio);
-            if (P.gnn) c.ms_gnn += tm.ms(4, 5);   // match_level has synchronized the stream
+            if (scored) c.ms_gnn += tm.ms(4, 5);   // match_level has synchronized the stream
             const int64_t n = lv.back().g.n;
             if (tr.on()) {
                 auto h = to_host(c, match, n);

@@ -45,6 +45,7 @@ struct gp_gnn {
     int64_t step = 0;
     float hedge[gp::ZD + 3] = {};     // host copy of the BF16-rounded A, beta, gamma, delta
     int32_t prio_bits = 16;           // priority = rint(logit * 2^prio_bits) + 2^30
+    int32_t max_level = -1;           // learned priorities at levels <= max_level (-1: every level)
     gp::Arena arena;                  // per-vertex activations
     gp::Arena keep;                   // row buckets of graphs scored outside a V-cycle
 };
@@ -650,6 +651,8 @@ static void gnn_edges(Ctx& c, const gp_gnn* G, const Level& L, const GnnActs& A,
     c.bytes += 8 * (L.g.n + 1) + 4 * L.g.m * (2 + ZD + 1) + (L.g.ew ? 4 * L.g.m : 0) + 4 * L.g.n * (ZD + 1);
 }
 
+bool gnn_scores_level(const gp_gnn* G, int level) { return G->max_level < 0 || level <= G->max_level; }
+
 // learned matching priorities of one level (called by the V-cycle driver)
 void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, int32_t* prio) {
     auto mk = c.tmp->save();
@@ -821,6 +824,15 @@ int gp_gnn_set_prio_bits(gp_gnn* G, int32_t bits) {
 }
 
 int gp_gnn_get_prio_bits(const gp_gnn* G) { return G ? G->prio_bits : -1; }
+
+int gp_gnn_set_max_level(gp_gnn* G, int32_t level) {
+    return gnn_guard([&] {
+        if (!G || level < -1) throw GpError(GP_EINVAL, "max level must be >= -1");
+        G->max_level = level;
+    });
+}
+
+int gp_gnn_get_max_level(const gp_gnn* G) { return G ? G->max_level : -2; }
 
 int gp_gnn_get_params(const gp_gnn* G, float* params, int32_t np) {
     return gnn_guard([&] {

@@ -132,6 +132,7 @@ void initpart_smem_caps();
 
 // gp_gnn.cu
 void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, int32_t* prio);
+bool gnn_scores_level(const gp_gnn* G, int level);   // false: edge weights at this level
 
 // gp_coarsen.cu
 void build_heavy(Ctx& c, Level& L);

@@ -161,19 +161,23 @@ def validation_set(count_per_family: int = 2, seed: int = 1, n: int = 200_000, d
     return out
 
 
-def tune_prio_bits(model: GNN, graphs, k: int = 32, candidates=(4, 6, 8, 10, 12, 16), log=None):
-    """Set model.prio_bits to the candidate with the lowest geometric-mean
-    learned/plain cut ratio over `graphs`; returns {bits: ratio}."""
+def tune_prio_bits(model: GNN, graphs, k: int = 32, candidates=(4, 6, 8, 10, 12, 16), levels=(0, 1, -1), log=None):
+    """Set model.prio_bits and model.max_level to the candidate pair with the
+    lowest geometric-mean learned/plain cut ratio over `graphs`; returns
+    {(bits, max_level): ratio}."""
     plain = [partition(rp, ci, k)[1]["cut"] for rp, ci in graphs]
     res = {}
-    for b in candidates:
-        model.prio_bits = b
-        logs = [math.log(max(partition_learned(rp, ci, k, model, judge=False)[1]["cut"], 1) / max(c, 1))
-                for (rp, ci), c in zip(graphs, plain)]
-        res[b] = math.exp(sum(logs) / len(logs))
-        if log:
-            log(f"prio_bits {b}: geometric-mean cut ratio {res[b]:.4f}")
-    model.prio_bits = min(res, key=lambda b: (res[b], -b))
+    for lv in levels:
+        for b in candidates:
+            model.prio_bits = b
+            model.max_level = lv
+            logs = [math.log(max(partition_learned(rp, ci, k, model, judge=False)[1]["cut"], 1) / max(c, 1))
+                    for (rp, ci), c in zip(graphs, plain)]
+            res[(b, lv)] = math.exp(sum(logs) / len(logs))
+            if log:
+                log(f"prio_bits {b}, max_level {lv}: geometric-mean cut ratio {res[(b, lv)]:.4f}")
+    b, lv = min(res, key=lambda t: (res[t], -t[0]))
+    model.prio_bits, model.max_level = b, lv
     return res
 
 
@@ -221,6 +225,7 @@ def main(argv=None):
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--out", default="gnn_weights.npz")
     t.add_argument("--init", default=None, help="start from these weights instead of a seeded init")
+    t.add_argument("--tune-only", action="store_true", help="with --init: only re-tune prio_bits / max_level")
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=None)
     e.add_argument("--graphs", default="rmat22,grid3d256")
@@ -231,18 +236,19 @@ def main(argv=None):
     log = lambda s: print(s, flush=True)
     import torch
     if a.cmd == "train":
-        t0 = time.time()
-        samples = build_dataset(a.graphs, a.seed, log=log)
-        log(f"dataset: {len(samples)} samples, {sum(int(s[1].numel()) for s in samples)} entries, "
-            f"{time.time() - t0:.1f}s")
         model = GNN.load(a.init) if a.init else GNN(init_params(a.seed))
-        t1 = time.time()
-        hist = train(model, samples, a.epochs, a.batch, a.lr, a.seed, log=log)
-        log(f"training: {time.time() - t1:.1f}s, loss {hist[0]:.4f} -> {hist[-1]:.4f}")
-        del samples
-        torch.cuda.empty_cache()
+        if not (a.tune_only and a.init):
+            t0 = time.time()
+            samples = build_dataset(a.graphs, a.seed, log=log)
+            log(f"dataset: {len(samples)} samples, {sum(int(s[1].numel()) for s in samples)} entries, "
+                f"{time.time() - t0:.1f}s")
+            t1 = time.time()
+            hist = train(model, samples, a.epochs, a.batch, a.lr, a.seed, log=log)
+            log(f"training: {time.time() - t1:.1f}s, loss {hist[0]:.4f} -> {hist[-1]:.4f}")
+            del samples
+            torch.cuda.empty_cache()
         tune_prio_bits(model, validation_set(), log=log)
-        log(f"prio_bits = {model.prio_bits}")
+        log(f"prio_bits = {model.prio_bits}, max_level = {model.max_level}")
         model.save(a.out)
         log(f"saved {a.out}")
     else:
