@@ -822,8 +822,10 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
 
 // tier D split over CTAs: rows longer than TC_ROW are cut into pieces of
 // TD_PIECE entries, one CTA each, all pieces of a row sharing that row's
-// global table.  D1 inserts (first position kept as the largest deg - j by
-// atomicMax, so that a zero-filled table starts empty), D2 ballots the
+// global table.  D1 inserts: a 64-bit slot holds (key + 1) << 32 | (deg - j),
+// zero meaning empty; the claiming compare-and-swap stores the first
+// position seen, later copies of the key raise it by atomicMax (the largest
+// deg - j is the first occurrence), weights add up in a 32-bit array.  D2 ballots the
 // first-occurrence flags of each 32-entry word, a device-wide scan of the word
 // popcounts ranks the words of every row, D3 writes the first occurrences at
 // their ranks.  Same output as one CTA per row: unique neighbours in order of
@@ -837,18 +839,18 @@ struct TierD {
     const int32_t* prow;    // row of each piece
     const int64_t* pbeg;    // entry range of the piece within the row
     const int64_t* pend;
-    int32_t* keys;          // tables: keys (filled with EMPTY_KEY), first position, weight sum
-    int32_t* pos;
-    int32_t* wsum;
+    unsigned long long* slot;   // tables: (key + 1) << 32 | (deg - first position), 0 = empty
+    int32_t* wsum;              // weight sums
     uint32_t* bits;         // first-occurrence flags, one word per 32 entries
     int32_t* wcnt;          // their popcounts
     const int64_t* wpre;    // exclusive prefix of wcnt (+ total)
 };
 
-__device__ __forceinline__ uint32_t td_lookup(const int32_t* keys, int32_t cu, int lg) {
+__device__ __forceinline__ uint32_t td_lookup(const unsigned long long* slot, int32_t cu, int lg) {
     const uint32_t mask = (1u << lg) - 1u;
+    const uint32_t tag = (uint32_t)cu + 1u;
     uint32_t h = slot_hash(cu, lg);
-    for (uint32_t probe = 0; probe <= mask && keys[h] != cu; ++probe) h = (h + 1) & mask;
+    for (uint32_t probe = 0; probe <= mask && (uint32_t)(slot[h] >> 32) != tag; ++probe) h = (h + 1) & mask;
     return h;
 }
 
@@ -860,36 +862,38 @@ __global__ void __launch_bounds__(TD_T) k_td_insert(TierD D, const int64_t* __re
     const int32_t self = D.rc[r];
     const int lg = D.rlg[r];
     const uint32_t mask = (1u << lg) - 1u;
-    int32_t* keys = D.keys + D.rtab[r];
-    int32_t* pos = D.pos + D.rtab[r];
+    unsigned long long* slot = D.slot + D.rtab[r];
     int32_t* wsum = D.wsum + D.rtab[r];
     const int64_t o = off[self], deg = cdeg[self], end = D.pend[blockIdx.x];
     for (int64_t base = D.pbeg[blockIdx.x]; base < end; base += 4 * TD_T) {
-        int32_t cu[4], wt[4], old[4];
+        int32_t cu[4], wt[4];
+        unsigned long long val[4], old[4];
         uint32_t h[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int64_t j = base + c * TD_T + threadIdx.x;
             cu[c] = j < end ? __ldcs(&mapped[o + j]) : self;
             wt[c] = j < end ? __ldcs(&mw[o + j]) : 0;
+            val[c] = ((unsigned long long)((uint32_t)cu[c] + 1u) << 32) | (uint32_t)(deg - j);
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             h[c] = slot_hash(cu[c], lg);
-            old[c] = cu[c] != self ? atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]) : EMPTY_KEY;
+            old[c] = cu[c] != self ? atomicCAS(&slot[h[c]], 0ull, val[c]) : 0ull;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             if (cu[c] == self) continue;
+            const uint32_t tag = (uint32_t)cu[c] + 1u;
             uint32_t probe = 1;
-            while (old[c] != EMPTY_KEY && old[c] != cu[c] && probe <= mask) {
+            while (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag && probe <= mask) {
                 h[c] = (h[c] + 1) & mask;
-                old[c] = atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]);
+                old[c] = atomicCAS(&slot[h[c]], 0ull, val[c]);
                 ++probe;
             }
-            if (old[c] != EMPTY_KEY && old[c] != cu[c]) { atomicExch(err, 1); continue; }
-            const int64_t j = base + c * TD_T + threadIdx.x;
-            atomicMax(&pos[h[c]], (int32_t)(deg - j));
+            if (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag) { atomicExch(err, 1); continue; }
+            // claimed with this position, or the key was there: keep the earliest position
+            if (old[c] != 0ull && old[c] < val[c]) atomicMax(&slot[h[c]], val[c]);
             atomicAdd(&wsum[h[c]], wt[c]);
         }
     }
@@ -901,8 +905,7 @@ __global__ void __launch_bounds__(TD_T) k_td_flags(TierD D, const int64_t* __res
     const int32_t r = D.prow[blockIdx.x];
     const int32_t self = D.rc[r];
     const int lg = D.rlg[r];
-    const int32_t* keys = D.keys + D.rtab[r];
-    const int32_t* pos = D.pos + D.rtab[r];
+    const unsigned long long* slot = D.slot + D.rtab[r];
     const int64_t o = off[self], deg = cdeg[self];
     const int lane = threadIdx.x & 31;
     const int64_t w0 = D.pbeg[blockIdx.x] / 32, w1 = (D.pend[blockIdx.x] + 31) / 32;
@@ -911,7 +914,7 @@ __global__ void __launch_bounds__(TD_T) k_td_flags(TierD D, const int64_t* __res
         bool first = false;
         if (j < deg) {
             const int32_t cu = mapped[o + j];
-            if (cu != self) first = pos[td_lookup(keys, cu, lg)] == (int32_t)(deg - j);
+            if (cu != self) first = (uint32_t)slot[td_lookup(slot, cu, lg)] == (uint32_t)(deg - j);
         }
         const uint32_t word = __ballot_sync(0xffffffffu, first);
         if (lane == 0) {
@@ -928,7 +931,7 @@ __global__ void __launch_bounds__(TD_T) k_td_write(TierD D, const int64_t* __res
     const int32_t r = D.prow[blockIdx.x];
     const int32_t self = D.rc[r];
     const int lg = D.rlg[r];
-    const int32_t* keys = D.keys + D.rtab[r];
+    const unsigned long long* slot = D.slot + D.rtab[r];
     const int32_t* wsum = D.wsum + D.rtab[r];
     const int64_t o = off[self], deg = cdeg[self];
     const int64_t rw = D.rword[r], nwords = (deg + 31) / 32;
@@ -941,7 +944,7 @@ __global__ void __launch_bounds__(TD_T) k_td_write(TierD D, const int64_t* __res
         const int32_t cu = mapped[o + wi * 32 + lane];
         const int64_t rank = D.wpre[rw + wi] - D.wpre[rw] + __popc(word & lt);
         tci[o + rank] = cu;
-        tew[o + rank] = wsum[td_lookup(keys, cu, lg)];
+        tew[o + rank] = wsum[td_lookup(slot, cu, lg)];
     }
     if (D.pbeg[blockIdx.x] == 0 && threadIdx.x == 0) rowcnt[self] = (int32_t)(D.wpre[rw + nwords] - D.wpre[rw]);
 }
@@ -1069,15 +1072,14 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         GP_CUDA(cudaMemcpyAsync(d_pend, pend.data(), sizeof(int64_t) * np, cudaMemcpyHostToDevice, c.s));
         D.rc = d_rc; D.rlg = d_rlg; D.rtab = d_rtab; D.rword = d_rword;
         D.prow = d_prow; D.pbeg = d_pbeg; D.pend = d_pend;
-        D.keys = c.tmp_alloc<int32_t>(tab);
-        D.pos = c.tmp_alloc<int32_t>(2 * tab);
-        D.wsum = D.pos + tab;
+        D.slot = c.tmp_alloc<unsigned long long>(tab);
+        D.wsum = c.tmp_alloc<int32_t>(tab);
         D.bits = (uint32_t*)c.tmp_alloc<int32_t>(words);
         D.wcnt = c.tmp_alloc<int32_t>(words);
         int64_t* wpre = c.tmp_alloc<int64_t>(words + 1);
         D.wpre = wpre;
-        GP_CUDA(cudaMemsetAsync(D.keys, 0xff, sizeof(int32_t) * tab, c.s));
-        GP_CUDA(cudaMemsetAsync(D.pos, 0, sizeof(int32_t) * 2 * tab, c.s));
+        GP_CUDA(cudaMemsetAsync(D.slot, 0, sizeof(unsigned long long) * tab, c.s));
+        GP_CUDA(cudaMemsetAsync(D.wsum, 0, sizeof(int32_t) * tab, c.s));
         k_td_insert<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped, mw, err);
         GP_LAUNCHED(c);
         k_td_flags<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped);
