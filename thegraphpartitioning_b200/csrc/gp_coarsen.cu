@@ -715,46 +715,51 @@ __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_
     }
 }
 
-// tiers C and D: one CTA per row, two phases.  Phase 1 inserts every entry
-// (first position by atomicMin, weights by atomicAdd), four entries per
-// thread in flight.  Phase 2: warps ballot the first-position flags of 32
-// consecutive positions into one word each, one block scan over the word
-// popcounts gives each word's base rank, and a second strided sweep writes
-// the first occurrences at base + rank within the word.
-// words: 2 * ceil(deg/32) ints of scratch (bits, then prefix).
+// tier C: one CTA per row, table in shared memory, two phases.  Phase 1
+// inserts every entry into a 64-bit slot (key + 1) << 32 | (deg - j), zero
+// meaning empty: the claiming compare-and-swap stores the first position
+// seen, later copies raise it by atomicMax (the largest deg - j is the first
+// occurrence); weights add up in wsum.  Phase 2: warps ballot the
+// first-occurrence flags of 32 consecutive positions into one word each, one
+// block scan over the word popcounts gives each word's base rank, and a
+// second strided sweep writes the first occurrences at base + rank within
+// the word.  words: 2 * ceil(deg/32) ints of scratch (bits, then prefix).
 template <int T>
 __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw, int64_t o, int64_t deg,
-                          int32_t self, int32_t* keys, int32_t* minpos, int32_t* wsum, int64_t S, int lg,
+                          int32_t self, unsigned long long* slot, int32_t* wsum, int64_t S, int lg,
                           int32_t* words, int32_t* __restrict__ tci, int32_t* __restrict__ tew, int32_t* cnt_out,
                           int32_t* sh, int32_t* err) {
     const uint32_t mask = (uint32_t)(S - 1);
-    for (int64_t i = threadIdx.x; i < S; i += T) { keys[i] = EMPTY_KEY; minpos[i] = INT32_MAX; wsum[i] = 0; }
+    for (int64_t i = threadIdx.x; i < S; i += T) { slot[i] = 0ull; wsum[i] = 0; }
     __syncthreads();
     for (int64_t base = 0; base < deg; base += 4 * T) {
-        int32_t cu[4], wt[4], old[4];
+        int32_t cu[4], wt[4];
+        unsigned long long val[4], old[4];
         uint32_t h[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int64_t j = base + c * T + threadIdx.x;
             cu[c] = j < deg ? mapped[o + j] : self;
             wt[c] = j < deg ? mw[o + j] : 0;
+            val[c] = ((unsigned long long)((uint32_t)cu[c] + 1u) << 32) | (uint32_t)(deg - j);
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             h[c] = slot_hash(cu[c], lg);
-            old[c] = cu[c] != self ? atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]) : EMPTY_KEY;
+            old[c] = cu[c] != self ? atomicCAS(&slot[h[c]], 0ull, val[c]) : 0ull;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             if (cu[c] == self) continue;
+            const uint32_t tag = (uint32_t)cu[c] + 1u;
             int64_t probe = 1;
-            while (old[c] != EMPTY_KEY && old[c] != cu[c] && probe < S) {
+            while (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag && probe < S) {
                 h[c] = (h[c] + 1) & mask;
-                old[c] = atomicCAS(&keys[h[c]], EMPTY_KEY, cu[c]);
+                old[c] = atomicCAS(&slot[h[c]], 0ull, val[c]);
                 ++probe;
             }
-            if (old[c] != EMPTY_KEY && old[c] != cu[c]) { atomicExch(err, 1); continue; }
-            atomicMin(&minpos[h[c]], (int32_t)(base + c * T + threadIdx.x));
+            if (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag) { atomicExch(err, 1); continue; }
+            if (old[c] != 0ull && old[c] < val[c]) atomicMax(&slot[h[c]], val[c]);
             atomicAdd(&wsum[h[c]], wt[c]);
         }
     }
@@ -764,8 +769,9 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
     int32_t* bits = words;
     int32_t* wpre = words + nwords;
     auto lookup = [&](int32_t cu) -> uint32_t {
+        const uint32_t tag = (uint32_t)cu + 1u;
         uint32_t hh = slot_hash(cu, lg);
-        for (int64_t probe = 0; probe < S && keys[hh] != cu; ++probe) hh = (hh + 1) & mask;
+        for (int64_t probe = 0; probe < S && (uint32_t)(slot[hh] >> 32) != tag; ++probe) hh = (hh + 1) & mask;
         return hh;
     };
     for (int64_t wi = wid; wi < nwords; wi += nwarp) {
@@ -773,7 +779,7 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
         bool first = false;
         if (j < deg) {
             const int32_t cu = mapped[o + j];
-            if (cu != self) first = minpos[lookup(cu)] == (int32_t)j;
+            if (cu != self) first = (uint32_t)slot[lookup(cu)] == (uint32_t)(deg - j);
         }
         const uint32_t word = __ballot_sync(0xffffffffu, first);
         if (lane == 0) bits[wi] = (int32_t)word;
@@ -807,7 +813,10 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
                                                          const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
                                                          int32_t* __restrict__ tci, int32_t* __restrict__ tew,
                                                          int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
-    extern __shared__ int32_t stab[];
+    extern __shared__ __align__(16) unsigned char stab_raw[];
+    unsigned long long* slot = (unsigned long long*)stab_raw;          // TC_SLOTS
+    int32_t* wsum = (int32_t*)(slot + TC_SLOTS);                       // TC_SLOTS
+    int32_t* words = wsum + TC_SLOTS;                                  // 2 * TC_ROW / 32
     __shared__ int32_t sh[33];
     for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int64_t c = list[li];
@@ -815,8 +824,7 @@ __global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restri
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg) { S <<= 1; ++lg; }
-        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, stab, stab + S, stab + 2 * S, S, lg, stab + 3 * TC_SLOTS,
-                        tci, tew, &cnt[c], sh, err);
+        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, slot, wsum, S, lg, words, tci, tew, &cnt[c], sh, err);
     }
 }
 
@@ -1022,7 +1030,7 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     c.sync();
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
     if (nC > 0) {
-        const size_t smem = sizeof(int32_t) * (3 * TC_SLOTS + 2 * ((TC_ROW + 31) / 32));
+        const size_t smem = (sizeof(unsigned long long) + sizeof(int32_t)) * TC_SLOTS + sizeof(int32_t) * 2 * ((TC_ROW + 31) / 32);
         k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * 2), TC_T, smem, c.s>>>(
             listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
@@ -1116,7 +1124,7 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
 void coarsen_smem_caps() {
     constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
     constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
-    const size_t smC = sizeof(int32_t) * (3 * TC_SLOTS + 2 * ((TC_ROW + 31) / 32));
+    const size_t smC = (sizeof(unsigned long long) + sizeof(int32_t)) * TC_SLOTS + sizeof(int32_t) * 2 * ((TC_ROW + 31) / 32);
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smA));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>,
