@@ -68,9 +68,11 @@ __device__ void ip_bfs(const DGraph& g, const int32_t* lab, int32_t* dist, const
     __syncthreads();
 }
 
+// labels and distances live in shared memory when they fit (on_chip), else in
+// the trial's slices of the global arrays; the kept labels are written out
 __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t seed, int32_t* __restrict__ labels,
                                                     int32_t* __restrict__ dists, int64_t* __restrict__ tcut,
-                                                    int64_t* __restrict__ tmaxpw, int key_iters) {
+                                                    int64_t* __restrict__ tmaxpw, int key_iters, int on_chip) {
     extern __shared__ int64_t ipsm[];
     __shared__ int flags[3];
     __shared__ int any;
@@ -86,8 +88,14 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
         int32_t* q = (int32_t*)p;
         S.cnt = q; q += k; S.cnt_d = q; q += k; S.incl = q; q += k;
     }
-    int32_t* lab = labels + (int64_t)t * n;
+    int32_t* glab = labels + (int64_t)t * n;
+    int32_t* lab = glab;
     int32_t* dist = dists + (int64_t)t * n;
+    if (on_chip) {
+        int32_t* q = (int32_t*)(ipsm + 9 * (int64_t)k) + 3 * (int64_t)k;
+        lab = q;
+        dist = q + n;
+    }
     const uint64_t ts = trial_salt(seed, t);
     for (int64_t v = threadIdx.x; v < n; v += blockDim.x) lab[v] = 0;
     for (int q = threadIdx.x; q < k; q += blockDim.x) S.cnt[q] = (q == 0) ? k : 0;
@@ -213,6 +221,8 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
         tcut[t] = s / 2;
         tmaxpw[t] = mp;
     }
+    if (on_chip)
+        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) glab[v] = lab[v];
 }
 
 __global__ void k_pick_trial(int T, const int64_t* __restrict__ tcut, const int64_t* __restrict__ tmaxpw, int64_t Lmax,
@@ -236,6 +246,8 @@ static int bits_for64(int64_t x) {
     return b;
 }
 
+size_t initpart_smem_max();
+
 int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out) {
     const int64_t n = L.g.n;
     const int T = P.o.init_trials;
@@ -245,9 +257,12 @@ int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out
     int64_t* tcut = c.tmp_alloc<int64_t>(T);
     int64_t* tmaxpw = c.tmp_alloc<int64_t>(T);
     int64_t* best = c.tmp_alloc<int64_t>(1);
-    const size_t smem = (size_t)P.k * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
+    const size_t base = (size_t)P.k * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
+    const size_t onchip = base + 2 * sizeof(int32_t) * (size_t)n;
+    const bool on_chip = onchip <= initpart_smem_max();
+    const size_t smem = on_chip ? onchip : base;
     const int key_iters = bits_for64(n * (n + 1)) + 1;
-    k_initpart<<<T, IP_T, smem, c.s>>>(L.g, P.k, P.seed, labels, dists, tcut, tmaxpw, key_iters);
+    k_initpart<<<T, IP_T, smem, c.s>>>(L.g, P.k, P.seed, labels, dists, tcut, tmaxpw, key_iters, on_chip ? 1 : 0);
     GP_LAUNCHED(c);
     k_pick_trial<<<1, 32, 0, c.s>>>(T, tcut, tmaxpw, P.Lmax, best);
     GP_LAUNCHED(c);
@@ -258,11 +273,22 @@ int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out
     return bt;
 }
 
-// the per-label arrays of k_initpart for the largest k; set once per device
-// (the cap is per kernel, shared by every thread of the process)
+// k_initpart may use the whole opt-in shared memory of a block (per-label
+// arrays, plus labels and distances when they fit); set once per device (the
+// cap is per kernel, shared by every thread of the process)
+static size_t g_ip_smem_max = 0;
+
+size_t initpart_smem_max() { return g_ip_smem_max; }
+
 void initpart_smem_caps() {
-    const size_t smem = (size_t)GP_MAX_K * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
-    GP_CUDA(cudaFuncSetAttribute(k_initpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, optin = 0;
+    GP_CUDA(cudaGetDevice(&dev));
+    GP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t need = (size_t)GP_MAX_K * (9 * sizeof(int64_t) + 3 * sizeof(int32_t));
+    // static shared memory of the kernel (flags, reductions) stays outside the cap
+    const size_t cap = std::max(need, (size_t)optin > 4096 ? (size_t)optin - 4096 : need);
+    GP_CUDA(cudaFuncSetAttribute(k_initpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
+    g_ip_smem_max = cap;
 }
 
 }  // namespace gp
