@@ -72,10 +72,13 @@ typedef struct gp_options {
                                    one thread block, one launch per level; 0 or < 0:
                                    off.  Results are identical either way; it pays
                                    only where launches, not SMs, are scarce            */
-    int32_t ctas_per_sm;        /* grid of the neighbour-scan kernels (matching rounds,
-                                   connectivity pass, afterburner): this many 256-thread
-                                   CTAs per SM at most (0: 8); results are identical for
-                                   every value (tuning knob of the autotuner)          */
+    int32_t ctas_per_sm;        /* grid of the row-scanning kernels (matching rounds,
+                                   contraction, connectivity pass, afterburner, cut): this
+                                   many CTAs per SM at most (0: 64 for one graph, where
+                                   many small work ranges balance better than a few
+                                   large ones; 8 in gp_partition_batch_device, where
+                                   concurrent V-cycles share the GPU); results are
+                                   identical for every value (autotuner knob)          */
     int32_t reserved[2];
 } gp_options;
 

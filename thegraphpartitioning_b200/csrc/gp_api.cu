@@ -225,6 +225,7 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
     P.gnn = gnn;
     resolve_options(opt, k, &P.o);
     P.k = k; P.seed = seed; P.imbalance = imbalance;
+    c.ctas_per_sm = P.o.ctas_per_sm;
     Timer tm;
     c.profile = P.o.profile > 0;
     if (c.profile) { c.ev_a = tm.e[6]; c.ev_b = tm.e[7]; }

@@ -74,6 +74,13 @@ extern "C" int gp_partition_batch_device(int32_t ngraphs, const int64_t* ns, con
             if (ms[i] < 0) throw GpError(GP_EINVAL, "negative entry count of graph " + std::to_string(i));
         }
         if (workers <= 0) workers = 16;
+        // concurrent V-cycles share the GPU: small grids per launch overlap
+        // better than the single-graph default (unless the caller chose)
+        gp_options bopt;
+        if (opt) bopt = *opt;
+        else { memset(&bopt, 0, sizeof bopt); bopt.version = GP_OPTIONS_VERSION; }
+        if (bopt.ctas_per_sm <= 0) bopt.ctas_per_sm = 8;
+        opt = &bopt;
         workers = std::min<int32_t>(workers, ngraphs);
         int dev = 0;
         GP_CUDA(cudaGetDevice(&dev));

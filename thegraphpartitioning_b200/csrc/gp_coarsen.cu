@@ -447,7 +447,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
         // nobody left who can propose: this round would add no pair
         if (units == 0 && heavy_live == 0) { rounds = r + 1; break; }
-        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * P.o.ctas_per_sm);
+        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * c.ctas_per_sm);
         memset_async(c, d_cnt, 0, 5 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);
@@ -480,7 +480,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
         const int64_t units = (B2.nlist[0] + 3) / 4 + B2.nlist[1] + B2.nlist[2];
-        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * 8);
+        const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * c.ctas_per_sm);
         k_match_scan<1><<<grid, 256, 0, c.s>>>(B2);
         GP_LAUNCHED(c);
         c.bytes += L.scan_bytes() + 4 * g.n;
@@ -1008,7 +1008,7 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     memset_async(c, lcount, 0, 3 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
-        const int grid = (int)fine.nitems + grid_for(g.n * 32, 256, c.sm_count * 8);
+        const int grid = (int)fine.nitems + grid_for(g.n * 32, 256, c.sm_count * c.ctas_per_sm);
         k_fill_mapped<<<grid, 256, 0, c.s>>>(g, fine.heavy, fine.item_row, fine.item_beg, fine.item_end, fine.nitems,
                                              fine.cmap, mem, off, mapped, mw);
         GP_LAUNCHED(c);
@@ -1018,9 +1018,9 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
         auto kA = k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>;
         auto kB = k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>;
-        kA<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, smA, c.s>>>(nc, 0, off, cdeg, mapped, mw, tci, tew, rowcnt);
+        kA<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, smA, c.s>>>(nc, 0, off, cdeg, mapped, mw, tci, tew, rowcnt);
         GP_LAUNCHED(c);
-        kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * 6), TB_WARPS * 32, smB, c.s>>>(nc, TA_ROW + 1, off, cdeg,
+        kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * c.ctas_per_sm), TB_WARPS * 32, smB, c.s>>>(nc, TA_ROW + 1, off, cdeg,
                                                                                         mapped, mw, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
@@ -1105,7 +1105,7 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     if ((int32_t)c.h_pinned[1] != 0) throw GpError(GP_EINTERNAL, "contraction hash table overflow");
     int32_t* cci = c.keep_alloc<int32_t>(mc);
     int32_t* cew = c.keep_alloc<int32_t>(mc);
-    k_contract_copy<<<grid_for(nc * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(nc, off, crp, tci, tew, cci, cew);
+    k_contract_copy<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, 0, c.s>>>(nc, off, crp, tci, tew, cci, cew);
     GP_LAUNCHED(c);
     // rows read twice (count and rank for long rows), cmap gathered per entry,
     // unique entries written to the temporary and copied once

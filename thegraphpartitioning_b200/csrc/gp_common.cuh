@@ -141,6 +141,7 @@ struct Ctx {
     int64_t launches = 0;
     int64_t bytes = 0;         // algorithmic bytes of executed passes
     int sm_count = 148;
+    int ctas_per_sm = 64;         // grid cap of row-scanning kernels, CTAs per SM (gp_options.ctas_per_sm)
     int64_t* h_pinned = nullptr;  // small pinned staging buffer (64 int64)
     // opt-in timing of the connectivity pass
     bool profile = false;

@@ -69,7 +69,7 @@ inline void resolve_options(const gp_options* in, int32_t k, gp_options* o) {
     if (d.lp_filter_den <= 0) d.lp_filter_den = 4;
     if (d.strong_after <= 0) d.strong_after = 2;
     if (d.check_input == 0) d.check_input = 1;
-    if (d.ctas_per_sm <= 0) d.ctas_per_sm = 8;
+    if (d.ctas_per_sm <= 0) d.ctas_per_sm = 64;
     *o = d;
 }
 

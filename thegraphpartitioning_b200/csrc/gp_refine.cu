@@ -749,7 +749,7 @@ void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64
 
 void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw) {
     memset_async(c, d_cross2, 0, sizeof(int64_t));
-    k_cut<<<grid_for(g.n * 32, RT, c.sm_count * 8), RT, 0, c.s>>>(g, part, d_cross2);
+    k_cut<<<grid_for(g.n * 32, RT, c.sm_count * c.ctas_per_sm), RT, 0, c.s>>>(g, part, d_cross2);
     GP_LAUNCHED(c);
     c.bytes += 8 * (g.n + 1) + 8 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.n;
     if (d_pw) part_weights(c, g, part, k, d_pw);
@@ -1231,7 +1231,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const int kpad = (k + 15) & ~15;
     const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
     // at most 1024 + 32 * GP_MAX_K bytes: below the 48 KB default, no attribute needed
-    const int light_blocks = grid_for(n * 32, RT, c.sm_count * P.o.ctas_per_sm);
+    const int light_blocks = grid_for(n * 32, RT, c.sm_count * c.ctas_per_sm);
     const int grid = (int)L.nitems + light_blocks;
     int64_t best_cut = 0, best_mp = 0;
     int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
