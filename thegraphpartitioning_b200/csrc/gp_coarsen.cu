@@ -1031,7 +1031,8 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
     if (nC > 0) {
         const size_t smem = (sizeof(unsigned long long) + sizeof(int32_t)) * TC_SLOTS + sizeof(int32_t) * 2 * ((TC_ROW + 31) / 32);
-        k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * 2), TC_T, smem, c.s>>>(
+        // one CTA per row: the block scheduler balances rows of unequal length
+        k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * c.ctas_per_sm), TC_T, smem, c.s>>>(
             listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
