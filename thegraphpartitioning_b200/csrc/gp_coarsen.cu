@@ -190,6 +190,8 @@ struct MatchArgs {
     int nbits;
     const int32_t* prio;      // learned priorities per entry (nullptr: edge weights)
     const uint8_t* hdead;     // MODE 0: heavy rows left without an eligible neighbour (nullptr: none)
+    int any_matched;          // MODE 0: 0 in the first round (no neighbour to look up in match[])
+    int check_vw;             // MODE 0: 0 when no two vertices of the level can exceed maxvw
 };
 
 // high word of an entry's matching priority: learned score or edge weight
@@ -201,8 +203,8 @@ template <int MODE>
 __device__ __forceinline__ bool match_ok(const MatchArgs& A, int64_t v, int32_t u, int64_t vwv) {
     if (u == (int32_t)v) return false;
     if (MODE == 0) {
-        if (A.match[u] != -1) return false;
-        if (vwv + (A.g.vw ? A.g.vw[u] : 1) > A.maxvw) return false;
+        if (A.any_matched && A.match[u] != -1) return false;
+        if (A.check_vw && vwv + (A.g.vw ? A.g.vw[u] : 1) > A.maxvw) return false;
     }
     return true;
 }
@@ -324,14 +326,14 @@ __global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        mm[c] = (MODE == 0 && uu[c] >= 0) ? A.match[uu[c]] : -1;
-                        vv[c] = (MODE == 0 && uu[c] >= 0 && A.g.vw) ? A.g.vw[uu[c]] : 1;
+                        mm[c] = (MODE == 0 && A.any_matched && uu[c] >= 0) ? A.match[uu[c]] : -1;
+                        vv[c] = (MODE == 0 && A.check_vw && uu[c] >= 0 && A.g.vw) ? A.g.vw[uu[c]] : 1;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const int32_t x = uu[c];
                         if (x < 0 || x == (int32_t)v) continue;
-                        if (MODE == 0 && (mm[c] != -1 || vwv + vv[c] > A.maxvw)) continue;
+                        if (MODE == 0 && (mm[c] != -1 || (A.check_vw && vwv + vv[c] > A.maxvw))) continue;
                         argmax_merge(bk, bid, edge_key(ww[c], edge_hash(A.salt, (int32_t)v, x)), x);
                     }
                 }
@@ -417,6 +419,14 @@ static int bits_for(int64_t x) {  // bits to represent values in [0, x)
     return b;
 }
 
+__global__ void k_max_vw(int64_t n, const int32_t* __restrict__ vw, int64_t* __restrict__ out) {
+    int32_t mx = 0;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        mx = vw[v] > mx ? vw[v] : mx;
+    for (int o = 16; o > 0; o >>= 1) { const int32_t y = __shfl_xor_sync(0xffffffffu, mx, o); mx = y > mx ? y : mx; }
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax((unsigned long long*)out, (unsigned long long)mx);
+}
+
 int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out,
                     const int32_t* prio) {
     const DGraph& g = L.g;
@@ -437,6 +447,18 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     A.hdone = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nheavy, 1));
     memset_async(c, A.hdone, 0, sizeof(int32_t) * std::max<int64_t>(L.nheavy, 1));
     A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0; A.prio = prio;
+    // weight cap: skip the per-neighbour weight check when the two heaviest
+    // vertices of the level together stay within maxvw
+    A.check_vw = 0;
+    if (g.vw) {
+        int64_t* d_mx = c.tmp_alloc<int64_t>(1);
+        memset_async(c, d_mx, 0, sizeof(int64_t));
+        k_max_vw<<<grid_for(g.n, 256, c.sm_count * 4), 256, 0, c.s>>>(g.n, g.vw, d_mx);
+        GP_LAUNCHED(c);
+        A.check_vw = 2 * read_i64(c, d_mx) > P.maxvw ? 1 : 0;
+    } else {
+        A.check_vw = 2 > P.maxvw ? 1 : 0;
+    }
     uint8_t* hdead = c.tmp_alloc<uint8_t>(std::max<int64_t>(L.nheavy, 1));
     memset_async(c, hdead, 0, std::max<int64_t>(L.nheavy, 1));
     A.hdead = hdead;
@@ -447,6 +469,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
         // nobody left who can propose: this round would add no pair
         if (units == 0 && heavy_live == 0) { rounds = r + 1; break; }
+        A.any_matched = r > 0 ? 1 : 0;
         const int grid = (int)L.nitems + grid_for(units * 32, 256, c.sm_count * c.ctas_per_sm);
         memset_async(c, d_cnt, 0, 5 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
@@ -477,6 +500,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         memset_async(c, d_cnt, 0, 2 * sizeof(int64_t));
         MatchArgs B2 = A;
         B2.hdead = nullptr;   // anchors: the top neighbour over all neighbours
+        B2.any_matched = 1;
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
         const int64_t units = (B2.nlist[0] + 3) / 4 + B2.nlist[1] + B2.nlist[2];
