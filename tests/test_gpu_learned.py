@@ -179,3 +179,31 @@ def test_trained_model_against_plain(gp, cuda):
         assert r["ms_gnn"] <= 0.2 * r["ms_plain"] + 10.0, r
         rows.append((name, r["cut_plain"], r["cut_learned"], round(r["cut_ratio"], 4), round(r["time_ratio"], 3)))
     print("\nlearned vs plain (k=32):", rows)
+
+
+def test_learned_api_rejects_invalid(gp, cuda):
+    """Invalid arguments return GP_EINVAL with a message; the context stays usable."""
+    import ctypes as C
+    from thegraphpartitioning_b200._abi import GP_EINVAL
+    L = gp.lib()
+    model = gp.GNN(learned.init_params(0))
+    with pytest.raises(gp.GPError) as e:
+        model.set_params(np.zeros(10, dtype=np.float32))
+    assert e.value.code == GP_EINVAL
+    with pytest.raises(gp.GPError):
+        model.prio_bits = 17
+    with pytest.raises(gp.GPError):
+        model.max_level = -2
+    assert model.prio_bits == 16 and model.max_level == -1
+    rp, ci = graphs.grid2d(20, 20)
+    rp, ci = rp.to(cuda), ci.to(cuda)
+    part = torch.empty(rp.numel() - 1, dtype=torch.int32, device=cuda)
+    rc = L.gp_partition_learned_device(rp.numel() - 1, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()), None,
+                                       None, 4, 0.03, 0, C.c_void_p(part.data_ptr()), None, None, None, None, 1, None,
+                                       None, None)
+    assert rc == GP_EINVAL and b"model" in L.gp_last_error()
+    with pytest.raises(gp.GPError):
+        gp.partition_learned(rp, ci, 0, model)
+    # still usable
+    p, st, rep, _ = gp.partition_learned(rp, ci, 4, model, judge=True)
+    assert st["cut"] == gp.edge_cut(rp, ci, p, 4)[0]
