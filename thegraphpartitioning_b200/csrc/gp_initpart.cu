@@ -39,6 +39,17 @@ struct IpShared {
     int64_t* xw;
 };
 
+// Adds w to sum[L] for every lane of the warp, one shared-memory atomic per
+// distinct label in the warp (lanes of one label are combined by match_any +
+// reduce).  L < 0: the lane adds nothing.  Exact: a label's weights total at
+// most the graph's vertex weight, which fits in 32 bits.
+__device__ __forceinline__ void ip_label_add(int64_t* sum, int32_t L, uint32_t w) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, (uint32_t)L);
+    const uint32_t tot = __reduce_add_sync(peers, L >= 0 ? w : 0u);
+    const int lane = threadIdx.x & 31;
+    if (L >= 0 && lane == __ffs(peers) - 1 && tot) atomicAdd((unsigned long long*)&sum[L], (unsigned long long)tot);
+}
+
 __device__ __forceinline__ int64_t ip_key(int32_t d, int64_t v, int64_t n) {
     return (int64_t)(d == IP_INF ? n : d) * n + v;
 }
@@ -111,11 +122,13 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
         __syncthreads();
         if (!any) break;
         const uint64_t ds = depth_salt(ts, d);
-        // label weights and seeds
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-            const int32_t L = lab[v];
-            if (S.cnt_d[L] <= 1) continue;
-            atomicAdd((unsigned long long*)&S.WL[L], (unsigned long long)(g.vw ? g.vw[v] : 1));
+        // label weights and seeds (warp-uniform trip count for the label sums)
+        for (int64_t v0 = threadIdx.x & ~31; v0 < n; v0 += blockDim.x) {
+            const int64_t v = v0 + (threadIdx.x & 31);
+            int32_t L = v < n ? lab[v] : -1;
+            if (L >= 0 && S.cnt_d[L] <= 1) L = -1;
+            ip_label_add(S.WL, L, L >= 0 ? (uint32_t)(g.vw ? g.vw[v] : 1) : 0u);
+            if (L < 0) continue;
             const uint64_t h = ((mix64(ds ^ (uint64_t)(uint32_t)v) >> 32) << 32) | (uint32_t)v;
             atomicMin((unsigned long long*)&S.s0[L], (unsigned long long)h);
         }
@@ -156,12 +169,13 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
         for (int it = 0; it < key_iters; ++it) {
             for (int q = threadIdx.x; q < k; q += blockDim.x) S.fsum[q] = 0;
             __syncthreads();
-            for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-                const int32_t L = lab[v];
-                if (S.cnt_d[L] <= 1) continue;
-                const int64_t mid = (S.lo[L] + S.hi[L]) >> 1;
-                if (ip_key(dist[v], v, n) < mid)
-                    atomicAdd((unsigned long long*)&S.fsum[L], (unsigned long long)(g.vw ? g.vw[v] : 1));
+            for (int64_t v0 = threadIdx.x & ~31; v0 < n; v0 += blockDim.x) {
+                const int64_t v = v0 + (threadIdx.x & 31);
+                int32_t L = v < n ? lab[v] : -1;
+                if (L >= 0 && S.cnt_d[L] <= 1) L = -1;
+                bool below = false;
+                if (L >= 0) below = ip_key(dist[v], v, n) < ((S.lo[L] + S.hi[L]) >> 1);
+                ip_label_add(S.fsum, below ? L : -1, below ? (uint32_t)(g.vw ? g.vw[v] : 1) : 0u);
             }
             __syncthreads();
             for (int q = threadIdx.x; q < k; q += blockDim.x) {
