@@ -50,6 +50,25 @@ __device__ __forceinline__ void ip_label_add(int64_t* sum, int32_t L, uint32_t w
     if (L >= 0 && lane == __ffs(peers) - 1 && tot) atomicAdd((unsigned long long*)&sum[L], (unsigned long long)tot);
 }
 
+// atomicMin (MAX = false) or atomicMax (MAX = true) of 64-bit keys into
+// slot[L], one shared-memory atomic per distinct label in the warp.  L < 0:
+// the lane takes no part.
+template <bool MAX>
+__device__ __forceinline__ void ip_label_ext(uint64_t* slot, int32_t L, uint64_t key) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, (uint32_t)L);
+    const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
+    const uint32_t ident = MAX ? 0u : 0xffffffffu;
+    const uint32_t bh = MAX ? __reduce_max_sync(peers, L >= 0 ? hi : ident) : __reduce_min_sync(peers, L >= 0 ? hi : ident);
+    const uint32_t cand = (L >= 0 && hi == bh) ? lo : ident;
+    const uint32_t bl = MAX ? __reduce_max_sync(peers, cand) : __reduce_min_sync(peers, cand);
+    const int lane = threadIdx.x & 31;
+    if (L >= 0 && lane == __ffs(peers) - 1) {
+        const unsigned long long best = ((unsigned long long)bh << 32) | bl;
+        if (MAX) atomicMax((unsigned long long*)&slot[L], best);
+        else atomicMin((unsigned long long*)&slot[L], best);
+    }
+}
+
 __device__ __forceinline__ int64_t ip_key(int32_t d, int64_t v, int64_t n) {
     return (int64_t)(d == IP_INF ? n : d) * n + v;
 }
@@ -128,9 +147,8 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
             int32_t L = v < n ? lab[v] : -1;
             if (L >= 0 && S.cnt_d[L] <= 1) L = -1;
             ip_label_add(S.WL, L, L >= 0 ? (uint32_t)(g.vw ? g.vw[v] : 1) : 0u);
-            if (L < 0) continue;
-            const uint64_t h = ((mix64(ds ^ (uint64_t)(uint32_t)v) >> 32) << 32) | (uint32_t)v;
-            atomicMin((unsigned long long*)&S.s0[L], (unsigned long long)h);
+            const uint64_t h = L >= 0 ? (((mix64(ds ^ (uint64_t)(uint32_t)v) >> 32) << 32) | (uint32_t)v) : ~0ull;
+            ip_label_ext<false>(S.s0, L, h);
         }
         __syncthreads();
         // BFS 1 from the seed
@@ -142,11 +160,12 @@ __global__ void __launch_bounds__(IP_T) k_initpart(DGraph g, int32_t k, uint64_t
         __syncthreads();
         ip_bfs(g, lab, dist, S, flags);
         // pseudo-peripheral vertex: max distance, smallest id
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-            const int32_t L = lab[v];
-            if (S.cnt_d[L] <= 1 || dist[v] == IP_INF) continue;
-            const uint64_t key = ((uint64_t)(uint32_t)dist[v] << 32) | (uint64_t)(0xffffffffu - (uint32_t)v);
-            atomicMax((unsigned long long*)&S.pk[L], (unsigned long long)key);
+        for (int64_t v0 = threadIdx.x & ~31; v0 < n; v0 += blockDim.x) {
+            const int64_t v = v0 + (threadIdx.x & 31);
+            int32_t L = v < n ? lab[v] : -1;
+            if (L >= 0 && (S.cnt_d[L] <= 1 || dist[v] == IP_INF)) L = -1;
+            const uint64_t key = L >= 0 ? (((uint64_t)(uint32_t)dist[v] << 32) | (uint64_t)(0xffffffffu - (uint32_t)v)) : 0ull;
+            ip_label_ext<true>(S.pk, L, key);
         }
         __syncthreads();
         for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
