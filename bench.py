@@ -174,37 +174,58 @@ def cpu_sample(args):
     }
 
 
+def _reference_worker(job):
+    """One host core: the oracle on the bounded R-MAT sample, `steps` timed
+    V-cycles after `warmup` untimed ones.  Returns (seconds per step, cut)."""
+    scale, seed, k, imbalance, steps, warmup = job
+    import oracle
+    rp, ci, _ = make_graph(scale, seed, "cpu")
+    rp_np, ci_np = rp.numpy(), ci.numpy()
+    for _ in range(warmup):
+        oracle.partition(rp_np, ci_np, k, imbalance, seed)
+    times, cut = [], None
+    for _ in range(steps):
+        t = time.perf_counter()
+        _, st, _ = oracle.partition(rp_np, ci_np, k, imbalance, seed)
+        times.append(time.perf_counter() - t)
+        cut = st["cut"]
+    return times, cut
+
+
 def run_reference(args, rank):
+    """The reference's path has no CPU implementation of its own (it is CUDA plus an
+    external gpmetis); its CPU counterpart is the oracle, the sequential restatement
+    of the same rules.  It is single-threaded, so the host's cores run independent
+    copies of the bounded sample at once (spawned processes), as the GPU arm runs
+    replicas: value = copies x edges x steps / slowest copy's time."""
     if rank != 0:
         return
+    import multiprocessing as mp
     import oracle
     oracle.build()
     rp, ci, _ = make_graph(args.sample_scale, args.seed, "cpu")
-    rp_np, ci_np = rp.numpy(), ci.numpy()
-    m = len(ci_np) // 2
-    for _ in range(args.warmup):
-        oracle.partition(rp_np, ci_np, args.k, args.imbalance, args.seed)
-    times = []
-    cut = None
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        _, st, _ = oracle.partition(rp_np, ci_np, args.k, args.imbalance, args.seed)
-        times.append(time.perf_counter() - t)
-        cut = st["cut"]
-    tot = sum(times)
-    value = m * args.steps / tot
-    sample = f"R-MAT scale {args.sample_scale} EF16 ({len(rp_np) - 1} vertices, {m} undirected edges), k={args.k}"
+    m = ci.numel() // 2
+    n = rp.numel() - 1
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    job = (args.sample_scale, args.seed, args.k, args.imbalance, args.steps, args.warmup)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_reference_worker, [job] * cores)
+    worst = max(sum(t) for t, _ in res)
+    cuts = {c for _, c in res}
+    value = cores * m * args.steps / worst
+    sample = (f"R-MAT scale {args.sample_scale} EF16 ({n} vertices, {m} undirected edges), k={args.k}, "
+              f"{cores} concurrent copies (one per host core)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * worst / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded R-MAT sample)",
         "config": {"workload": f"rmat{args.scale}_ef16_k{args.k}", "k": args.k, "imbalance": args.imbalance,
-                   "seed": args.seed, "timed_sample": sample, "cut": cut},
-        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample},
+                   "seed": args.seed, "timed_sample": sample, "cut": min(cuts), "copies_agree": len(cuts) == 1},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's path runs only on a GPU with an external gpmetis; its CPU counterpart "
-                "here is the oracle (sequential restatement of the same deterministic rules, 1 core)",
+                "here is the oracle (sequential restatement of the same deterministic rules), one copy per core",
     }
     print(json.dumps(line), flush=True)
 
