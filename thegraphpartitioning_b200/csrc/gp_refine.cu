@@ -812,11 +812,37 @@ __device__ int64_t cta_scan(int64_t cnt, F val, int64_t* out, int64_t* sh) {
     return tot;
 }
 
-// ascending bitonic sort of N (a power of two) unique keys in shared memory
+// ascending bitonic sort of N (a power of two) unique keys in shared memory.
+// Compare-exchange steps whose partner is within 16 positions run on
+// registers with warp shuffles (element i sits in lane i % 32 of its warp,
+// partner i ^ stride in the same warp); wider steps go through shared memory,
+// one block barrier each.
 __device__ void cta_bitonic(uint64_t* a, int N) {
-    for (int size = 2; size <= N; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < N; i += CT) {
+    const int tid = threadIdx.x;
+    const int E = N > CT ? N / CT : 1;
+    // strides top, top/2, ..., 1 of merge size `size` (size 0: every size 2..top*2)
+    auto warp_steps = [&](int size, int top) {
+        for (int e = 0; e < E; ++e) {
+            const int i = e * CT + tid;
+            const bool valid = i < N;
+            uint64_t x = valid ? a[i] : ~0ull;
+            const int s0 = size ? size : 2, s1 = size ? size : 2 * top;
+            for (int sz = s0; sz <= s1; sz <<= 1) {
+                for (int stride = size ? top : (sz >> 1); stride > 0; stride >>= 1) {
+                    const uint64_t y = __shfl_xor_sync(0xffffffffu, x, stride);
+                    const bool up = (i & sz) == 0, lower = (i & stride) == 0;
+                    x = (lower == up) ? (x < y ? x : y) : (x < y ? y : x);
+                }
+            }
+            if (valid) a[i] = x;
+        }
+        __syncthreads();
+    };
+    // merge sizes up to 32: within warps
+    warp_steps(0, (N < 32 ? N : 32) >> 1);
+    for (int size = 64; size <= N; size <<= 1) {
+        for (int stride = size >> 1; stride >= 32; stride >>= 1) {
+            for (int i = tid; i < N; i += CT) {
                 const int j = i ^ stride;
                 if (j > i) {
                     const uint64_t x = a[i], y = a[j];
@@ -826,6 +852,8 @@ __device__ void cta_bitonic(uint64_t* a, int N) {
             }
             __syncthreads();
         }
+        warp_steps(size, 16);
+    }
 }
 
 // first index in [0, i] whose key has the same segment (key >> shift) as key i
