@@ -23,6 +23,8 @@
 #include <chrono>
 #include <algorithm>
 #include <sys/stat.h>
+#include <thread>
+#include <charconv>
 
 #include <cuda_runtime.h>
 
@@ -39,7 +41,46 @@ bool file_exists(const std::string& p) {
     return stat(p.c_str(), &st) == 0 && S_ISREG(st.st_mode);
 }
 
-// Whitespace-separated integers of a text file.  max_count < 0: read all.
+inline bool is_space(char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t'; }
+
+// Number of tokens in buf[b, e) (b and e on token boundaries).
+size_t count_tokens(const char* buf, size_t b, size_t e) {
+    size_t c = 0;
+    bool in = false;
+    for (size_t i = b; i < e; ++i) {
+        const bool sp = is_space(buf[i]);
+        c += (!sp && !in) ? 1 : 0;
+        in = !sp;
+    }
+    return c;
+}
+
+// Integers of buf[b, e) written to out[first ..] (entries at or past `keep`
+// are dropped); on a malformed token, *bad = its index within the range.
+void parse_range(const char* buf, size_t b, size_t e, int64_t* out, size_t first, size_t keep, int64_t* bad) {
+    const char* p = buf + b;
+    const char* end = buf + e;
+    size_t i = 0;
+    *bad = -1;
+    while (p < end) {
+        while (p < end && is_space(*p)) ++p;
+        if (p >= end) break;
+        bool neg = false;
+        if (*p == '-') { neg = true; ++p; }
+        if (p >= end || *p < '0' || *p > '9') { *bad = (int64_t)i; return; }
+        int64_t v = 0;
+        while (p < end && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
+        if (p < end && !is_space(*p)) { *bad = (int64_t)i; return; }
+        if (first + i < keep) out[first + i] = neg ? -v : v;
+        ++i;
+    }
+}
+
+// Whitespace-separated integers of a text file, parsed by all host threads:
+// the file is cut into chunks at whitespace, a first pass counts each
+// chunk's integers, a second parses them straight into their final places.
+// max_count < 0: read all; otherwise the first max_count integers, and fewer
+// is an error (as readFile, src/gpu_part.cu:786-800).
 bool read_ints(const std::string& path, int64_t max_count, std::vector<int64_t>& out, std::string& err) {
     FILE* f = fopen(path.c_str(), "rb");
     if (!f) { err = "cannot open " + path; return false; }
@@ -50,20 +91,38 @@ bool read_ints(const std::string& path, int64_t max_count, std::vector<int64_t>&
     size_t got = fread(buf.data(), 1, (size_t)sz, f);
     fclose(f);
     buf[got] = 0;
-    out.clear();
-    if (max_count > 0) out.reserve((size_t)max_count);
-    const char* p = buf.data();
-    const char* end = p + got;
-    while (p < end && (max_count < 0 || (int64_t)out.size() < max_count)) {
-        while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) ++p;
-        if (p >= end) break;
-        bool neg = false;
-        if (*p == '-') { neg = true; ++p; }
-        if (p >= end || *p < '0' || *p > '9') { err = path + ": not an integer at element " + std::to_string(out.size()); return false; }
-        int64_t v = 0;
-        while (p < end && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
-        out.push_back(neg ? -v : v);
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    if (got < ((size_t)1 << 20)) nt = 1;
+    nt = std::min<unsigned>(nt, 64);
+    std::vector<size_t> cut(nt + 1), cnt(nt), first(nt + 1);
+    cut[0] = 0;
+    cut[nt] = got;
+    for (unsigned t = 1; t < nt; ++t) {
+        size_t b = got * t / nt;
+        if (b < cut[t - 1]) b = cut[t - 1];
+        while (b < got && !is_space(buf[b])) ++b;   // move to the end of the token
+        cut[t] = b;
     }
+    auto run = [&](auto&& fn) {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) th.emplace_back([&, t] { fn(t); });
+        for (auto& x : th) x.join();
+    };
+    run([&](unsigned t) { cnt[t] = count_tokens(buf.data(), cut[t], cut[t + 1]); });
+    first[0] = 0;
+    for (unsigned t = 0; t < nt; ++t) first[t + 1] = first[t] + cnt[t];
+    const size_t total = first[nt];
+    const size_t keep = max_count < 0 ? total : std::min<size_t>(total, (size_t)max_count);
+    out.resize(keep);
+    std::vector<int64_t> bad(nt, -1);
+    run([&](unsigned t) {
+        if (first[t] < keep) parse_range(buf.data(), cut[t], cut[t + 1], out.data(), first[t], keep, &bad[t]);
+    });
+    for (unsigned t = 0; t < nt; ++t)
+        if (bad[t] >= 0 && first[t] + (size_t)bad[t] < keep) {
+            err = path + ": not an integer at element " + std::to_string(first[t] + (size_t)bad[t]);
+            return false;
+        }
     if (max_count > 0 && (int64_t)out.size() < max_count) {
         err = "Error reading file " + path + " at element " + std::to_string(out.size());
         return false;
@@ -75,7 +134,7 @@ void usage(const char* a0) {
     fprintf(stderr,
             "Usage: %s <directory> <nvtxs> <nedges> <num_partitions> [options]\n"
             "   or: %s <row.txt> <column.txt> <num_partitions> [options]\n"
-            "options: --imbalance F  --seed N  --out FILE  --part-list FILE\n", a0, a0);
+            "options: --imbalance F  --seed N  --out FILE  --part-list FILE  --parse-only\n", a0, a0);
 }
 
 }  // namespace
@@ -85,6 +144,7 @@ int main(int argc, char** argv) {
     float imbalance = 0.03f;
     uint64_t seed = 0;
     std::string out_path = "./finalpartition.txt", part_list;
+    bool parse_only = false;   // read and check the input files only (no device work)
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
         auto need = [&](const char* name) -> const char* {
@@ -95,6 +155,7 @@ int main(int argc, char** argv) {
         else if (a == "--seed") seed = strtoull(need("--seed"), nullptr, 10);
         else if (a == "--out") out_path = need("--out");
         else if (a == "--part-list") part_list = need("--part-list");
+        else if (a == "--parse-only") parse_only = true;
         else if (a == "-h" || a == "--help") { usage(argv[0]); return 0; }
         else pos.push_back(a);
     }
@@ -136,6 +197,16 @@ int main(int argc, char** argv) {
     std::vector<int32_t> ci(ci64.begin(), ci64.end()), ew;
     if (have_w) ew.assign(ew64.begin(), ew64.end());
     const double t_read = now() - t0;
+    if (parse_only) {
+        uint64_t h = 1469598103934665603ull;   // FNV-1a over the parsed integers
+        auto mixin = [&](int64_t x) { h = (h ^ (uint64_t)x) * 1099511628211ull; };
+        for (int64_t x : rp) mixin(x);
+        for (int32_t x : ci) mixin(x);
+        for (int32_t x : ew) mixin(x);
+        printf("parsed n=%lld m=%lld weights=%d checksum=%016llx seconds=%.6f\n", (long long)n, (long long)ne,
+               have_w ? 1 : 0, (unsigned long long)h, t_read);
+        return 0;
+    }
 
     std::vector<int32_t> part((size_t)n);
     gp_stats st;
@@ -151,19 +222,36 @@ int main(int argc, char** argv) {
     const double t2 = now();
     std::vector<std::vector<int64_t>> by_part((size_t)k);
     for (int64_t v = 0; v < n; ++v) by_part[part[v]].push_back(v);
-    FILE* fo = fopen(out_path.c_str(), "w");
-    if (!fo) { fprintf(stderr, "Error: Cannot open %s for writing\n", out_path.c_str()); return 2; }
+    // formatted into one buffer (std::to_chars) and written at once
+    std::vector<char> obuf;
+    obuf.reserve((size_t)n * 9 + (size_t)k * 24);
+    auto put_int = [&](int64_t x) {
+        char tmp[24];
+        const auto r = std::to_chars(tmp, tmp + sizeof tmp, x);
+        obuf.insert(obuf.end(), tmp, r.ptr);
+    };
+    auto put_str = [&](const char* z) { obuf.insert(obuf.end(), z, z + strlen(z)); };
     for (int64_t q = 0; q < k; ++q) {
-        fprintf(fo, "Partition %lld: ", (long long)q);
+        put_str("Partition ");
+        put_int(q);
+        put_str(": ");
         const auto& vs = by_part[q];
-        for (size_t i = 0; i < vs.size(); ++i) fprintf(fo, i + 1 < vs.size() ? "%lld," : "%lld", (long long)vs[i]);
-        fputc('\n', fo);
+        for (size_t i = 0; i < vs.size(); ++i) {
+            put_int(vs[i]);
+            if (i + 1 < vs.size()) obuf.push_back(',');
+        }
+        obuf.push_back('\n');
     }
+    FILE* fo = fopen(out_path.c_str(), "wb");
+    if (!fo) { fprintf(stderr, "Error: Cannot open %s for writing\n", out_path.c_str()); return 2; }
+    fwrite(obuf.data(), 1, obuf.size(), fo);
     fclose(fo);
     if (!part_list.empty()) {
-        FILE* fp = fopen(part_list.c_str(), "w");
+        obuf.clear();
+        for (int64_t v = 0; v < n; ++v) { put_int(part[v]); obuf.push_back('\n'); }
+        FILE* fp = fopen(part_list.c_str(), "wb");
         if (!fp) { fprintf(stderr, "Error: Cannot open %s for writing\n", part_list.c_str()); return 2; }
-        for (int64_t v = 0; v < n; ++v) fprintf(fp, "%d\n", part[v]);
+        fwrite(obuf.data(), 1, obuf.size(), fp);
         fclose(fp);
     }
     const double t_write = now() - t2;
