@@ -134,3 +134,42 @@ def test_full_size_grid_config(oracle_mod, gp, cuda):
     p_gpu, s_gpu, _ = gp.partition(torch.from_numpy(rp).to(cuda), torch.from_numpy(ci).to(cuda), 4, 0.03, 0)
     assert np.array_equal(p_ref, p_gpu.cpu().numpy())
     assert s_gpu["max_part_weight"] <= s_gpu["max_allowed"]
+
+
+def _edge_cases():
+    # two vertices, two parts
+    yield "pair_k2", (np.array([0, 1, 2], np.int64), np.array([1, 0], np.int32)), 2, 0.0, None
+    # one part per vertex
+    rp, ci = to_np(*graphs.grid2d(5, 6))
+    yield "grid_k_eq_n", (rp, ci), 30, 0.03, None
+    # a clique
+    yield "clique50_k7", to_np(*graphs.cliques(1, 50)), 7, 0.03, None
+    # many components (2000 disjoint 4-cliques)
+    yield "components_k16", to_np(*graphs.cliques(2000, 4)), 16, 0.03, None
+    # a path (diameter = n - 1)
+    yield "path3000_k9", to_np(*graphs.path(3000)), 9, 0.03, None
+    # isolated vertices mixed in (Erdos-Renyi with mean degree 1)
+    yield "sparse_er_k5", to_np(*graphs.erdos_renyi(6000, 1.0, seed=3)), 5, 0.03, None
+    # heavy weights whose totals come close to the int32 limit
+    rp, ci = to_np(*graphs.grid2d(30, 30))
+    n = len(rp) - 1
+    ew = np.full(len(ci), 2 * 10**5, np.int32)
+    vw = np.full(n, 2 * 10**6, np.int32)
+    yield "heavy_weights_k6", (rp, ci), 6, 0.03, (ew, vw)
+
+
+ECASES = list(_edge_cases())
+
+
+@pytest.mark.parametrize("name,g,k,imb,w", ECASES, ids=[c[0] for c in ECASES])
+def test_edge_case_parity(oracle_mod, gp, cuda, name, g, k, imb, w):
+    rp, ci = g
+    ew, vw = (w if w is not None else (None, None))
+    p_ref, s_ref, ev_ref = oracle_mod.partition(rp, ci, k, imb, 3, vwgt=vw, ewgt=ew, trace=True)
+    d = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+    p_gpu, s_gpu, ev_gpu = gp.partition(d(rp), d(ci), k, imb, 3, vwgt=d(vw), ewgt=d(ew), trace=True)
+    compare_traces(ev_ref, ev_gpu)
+    assert np.array_equal(p_ref, p_gpu.cpu().numpy())
+    assert s_ref["cut"] == s_gpu["cut"] and s_ref["max_part_weight"] == s_gpu["max_part_weight"]
+    cut, pw = gp.edge_cut(d(rp), d(ci), p_gpu, k, ewgt=d(ew), vwgt=d(vw))
+    assert cut == s_gpu["cut"] and int(pw.max()) == s_gpu["max_part_weight"]
