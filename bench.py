@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--workload", default="rmat", choices=["rmat", "batch"],
                     help="rmat: one R-MAT graph (default); batch: the batched configuration")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--batch-stride", type=int, default=1,
+                    help="with --profile-once: take every stride-th graph of the 4096-graph batch")
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--autotune", action="store_true",
                     help="pick workers / launch-shape options on a sample first (untimed; results are identical)")
@@ -238,6 +240,25 @@ def run_batch(args, rank, world, dev, dist):
     import thegraphpartitioning_b200 as gp
     from thegraphpartitioning_b200 import graphs
     from thegraphpartitioning_b200._abi import make_options
+    if args.profile_once:
+        # one warm call, then one call between cudaProfilerStart/Stop, on a
+        # sample of the batch (every batch_stride-th graph, batch_count of them)
+        specs = graphs.batch_specs(4096, seed=args.seed)[::args.batch_stride][:args.batch_count]
+        gs = [graphs.batch_graph(sp, device=dev) for sp in specs]
+        ks = [sp["k"] for sp in specs]
+        seeds = [sp["seed"] for sp in specs]
+        gp.partition_batch(gs, ks, args.imbalance, seeds, workers=args.workers)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t = time.perf_counter()
+        _, st = gp.partition_batch(gs, ks, args.imbalance, seeds, workers=args.workers)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_once": "batch_sample", "graphs": len(gs), "stride": args.batch_stride,
+                          "workers": args.workers, "m": sum(g[1].numel() // 2 for g in gs), "seconds": dt,
+                          "launches": sum(x["kernel_launches"] for x in st)}), flush=True)
+        return
     specs = graphs.batch_specs(args.batch_count, seed=args.seed)
     # estimated cost n + m with m ~ n * mean degree / 2 for the shard assignment
     costs = [s["n"] * (1 + (4 if s["kind"] == "rgg" else 5)) for s in specs]
