@@ -13,7 +13,8 @@
 //               of the current state costs no extra pass), and the move proposal
 //               of the mode the device derives from the part weights
 //               (label propagation when no part exceeds Lmax, else rebalancing).
-//   LP:         k_copy_state + k_lp_apply: each candidate re-evaluates its gain
+//   LP:         k_lp_apply (the connectivity pass already copied part/lock into
+//               the next buffers): each candidate re-evaluates its gain
 //               against the proposals of higher-priority neighbours
 //               ((gain desc, id asc)) and moves when that gain is >= 0;
 //               double-buffered part/lock arrays, part-weight deltas aggregated
@@ -87,6 +88,8 @@ struct ConnArgs {
     int64_t nunits;
     int32_t* dest;
     int32_t* gain;
+    int32_t* part_next;         // label propagation: part and cleared lock copied here for the
+    uint8_t* lock_next;         // move step (nullptr: not needed)
     int64_t* status;
     int32_t* clist[3];
     int32_t* hhist;
@@ -113,6 +116,7 @@ __device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, i
 // and total weighted degree; returns true when an LP candidate is recorded
 __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool active, int64_t v, int32_t p,
                                             int64_t tot, int64_t cross, uint64_t bk, int32_t bq, int32_t light) {
+    if (mode == MODE_LP && A.part_next) { A.part_next[v] = p; A.lock_next[v] = 0; }
     const int64_t own = tot - cross;
     int32_t d = -1, gn = 0;
     bool cand = false;
@@ -405,14 +409,6 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
 }
 
 // ------------------------------------------------------------------ LP apply
-__global__ void k_copy_state(int64_t n, const int32_t* __restrict__ part, int32_t* __restrict__ part_next,
-                             uint8_t* __restrict__ lock_next) {
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        part_next[v] = part[v];
-        lock_next[v] = 0;
-    }
-}
-
 __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v, int32_t p, int32_t d, int32_t gv,
                                            const int32_t* __restrict__ part, const int32_t* __restrict__ dest,
                                            const int32_t* __restrict__ gain) {
@@ -1066,6 +1062,7 @@ __global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = R.bucket[b]; CA.nbucket[b] = R.nbucket[b]; CA.clist[b] = R.clist[b]; }
         CA.unit_cost = nullptr; CA.nunits = 0;
         CA.dest = R.dest; CA.gain = R.gain; CA.status = R.status;
+        CA.part_next = nullptr; CA.lock_next = nullptr;
         CA.hhist = nullptr; CA.hsum = nullptr; CA.hdone = nullptr;
         int64_t acc = 0;
         int32_t* hist = s_hist + w * k;
@@ -1277,6 +1274,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = L.bucket[b]; CA.nbucket[b] = L.nbucket[b]; CA.clist[b] = B.clist[b]; }
         CA.unit_cost = L.unit_cost; CA.nunits = L.nunits;
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
+        CA.part_next = B.part_next; CA.lock_next = B.lock_next;   // the LP step's starting copy
         k_conn<<<grid, RT, conn_smem, c.s>>>(CA);
         GP_LAUNCHED(c);
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_b, c.s));
@@ -1331,8 +1329,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         int64_t* moves_d = B.status + S_STEP_MOVES;  // moves of this step, read at the next sync
         memset_async(c, moves_d, 0, sizeof(int64_t));
         if (mode == 0) {
-            k_copy_state<<<grid_for(n, 256), 256, 0, c.s>>>(n, B.part, B.part_next, B.lock_next);
-            GP_LAUNCHED(c);
+            // part_next / lock_next were filled by the connectivity pass
             ApplyArgs AA;
             AA.g = g; AA.k = k; AA.part = B.part; AA.dest = B.dest; AA.gain = B.gain; AA.heavy = L.heavy;
             AA.item_row = L.item_row; AA.item_beg = L.item_beg; AA.item_end = L.item_end; AA.row_items = L.row_items;
