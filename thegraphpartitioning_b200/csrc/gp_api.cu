@@ -517,9 +517,7 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
             // the plain V-cycle into scratch; its result replaces the learned one
             // unless the learned partition is at least as balanced (within the
             // bound) and cuts no more
-            int32_t* plain = nullptr;
-            GP_CUDA(cudaMallocAsync(&plain, sizeof(int32_t) * n, c.s));
-            struct Free { int32_t* p; cudaStream_t s; ~Free() { cudaFreeAsync(p, s); } } fr{plain, c.s};
+            int32_t* plain = c.keep_alloc<int32_t>(n);   // the call's arena, like every other buffer
             gp_stats sp;
             Tracer none;
             run_vcycle(c, g, k, imbalance, seed, opt, plain, &sp, none);
