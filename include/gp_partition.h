@@ -197,7 +197,9 @@ int gp_partition_batch_device(int32_t ngraphs, const int64_t* ns, const int64_t*
 
 /* ---- learned matching priorities (no counterpart in the reference; its run
  * log names a GNNcoarsening.cu that is not in the repository) ------------- */
-typedef struct gp_gnn gp_gnn;   /* a small message-passing edge scorer, device resident */
+typedef struct gp_gnn gp_gnn;   /* a small message-passing edge scorer, device resident; its
+                                   scratch memory belongs to the handle, so one call at a time
+                                   per handle (use one handle per thread for concurrency) */
 
 int gp_gnn_num_params(void);
 int gp_gnn_create(gp_gnn** out);                 /* zero weights */
