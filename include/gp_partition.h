@@ -230,7 +230,7 @@ int gp_gnn_train_step_device(gp_gnn* model, int32_t ngraphs, const int64_t* ns, 
                              const uint8_t* const* d_labels, float lr, void* stream, float* loss_out);
 typedef struct gp_learned_report {
     int64_t cut_learned;              /* exact cut of the learned V-cycle             */
-    int64_t cut_plain;                /* exact cut of the plain V-cycle (judge != 0)   */
+    int64_t cut_plain;                /* exact cut of the plain V-cycle (fallback != 0)   */
     int64_t max_part_weight_learned;
     int64_t max_part_weight_plain;
     double  ms_learned;               /* device time of each V-cycle                   */
@@ -241,14 +241,14 @@ typedef struct gp_learned_report {
 } gp_learned_report;
 
 /* V-cycle whose matching priority at every level is the model's score instead
- * of the edge weight; all other rules unchanged.  judge != 0 also runs the
+ * of the edge weight; all other rules unchanged.  fallback != 0 also runs the
  * plain V-cycle and keeps the learned partition only when it is within the
  * balance bound (or the plain one is not) and its exact cut <= the plain cut;
  * stats describe the partition returned.  The trace covers the learned run. */
 int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
                                 const int32_t* d_vwgt, const int32_t* d_ewgt, int32_t k, float imbalance,
                                 uint64_t seed, int32_t* d_part_out, void* stream, const gp_options* opt,
-                                gp_stats* stats, const gp_gnn* model, int32_t judge, gp_learned_report* report,
+                                gp_stats* stats, const gp_gnn* model, int32_t fallback, gp_learned_report* report,
                                 gp_trace_fn trace, void* trace_user);
 
 /* Largest k accepted by gp_edge_cut_device_noalloc. */

@@ -6,7 +6,7 @@
   error of every parameter block below 2e-3 (FP32 accumulation);
 * the learned V-cycle is bit-exact against the oracle fed the same per-level
   priorities (every trace event compared);
-* training on the GPU reduces the loss; the judged mode never returns a cut
+* training on the GPU reduces the loss; the fallback mode never returns a cut
   above the plain one, and returns exactly the plain partition when it
   rejects the learned one.
 """
@@ -111,7 +111,7 @@ def test_learned_vcycle_matches_oracle(oracle_mod, gp, cuda):
             ew, vw = weighted(rp, ci, seed=7)
         model = gp.GNN(_params(3), prio_bits=10, max_level=max_level)
         part, st, rep, ev = gp.partition_learned(_dev(rp, cuda), _dev(ci, cuda), k, model, 0.03, seed,
-                                                 vwgt=_dev(vw, cuda), ewgt=_dev(ew, cuda), judge=False, trace=True)
+                                                 vwgt=_dev(vw, cuda), ewgt=_dev(ew, cuda), fallback=False, trace=True)
         prio = {e["level"]: e["a0"] for e in ev if e["kind"] == GP_TR_PRIO}
         assert prio and rep["kept_learned"] == 1
         if max_level >= 0:
@@ -143,13 +143,13 @@ def test_training_reduces_loss(gp, cuda):
     assert torch.equal(model.forward(s[0], s[1], s[2], s[3], s[4])[0], m2.forward(s[0], s[1], s[2], s[3], s[4])[0])
 
 
-def test_judged_mode_never_worse(gp, cuda):
+def test_fallback_mode_never_worse(gp, cuda):
     rp, ci = graphs.rmat(14, seed=9)[:2]
     rp, ci = rp.to(cuda), ci.to(cuda)
     plain, sp, _ = gp.partition(rp, ci, 32, 0.03, 2)
     for seed in (0, 1):
         model = gp.GNN(learned.init_params(seed))
-        part, st, rep, _ = gp.partition_learned(rp, ci, 32, model, 0.03, 2, judge=True)
+        part, st, rep, _ = gp.partition_learned(rp, ci, 32, model, 0.03, 2, fallback=True)
         assert rep["cut_plain"] == sp["cut"]
         assert st["cut"] <= sp["cut"]
         assert st["cut"] == gp.edge_cut(rp, ci, part, 32)[0]
@@ -163,7 +163,7 @@ def test_judged_mode_never_worse(gp, cuda):
                     reason="no trained weights")
 def test_trained_model_against_plain(gp, cuda):
     """What the trained scorer gains over plain heavy-edge matching on graphs
-    it was not trained on (k=32): the judged result is never worse, and the
+    it was not trained on (k=32): the result with the plain fallback is never worse, and the
     scorer's own inference costs at most a fifth of the plain V-cycle's device
     time (plus 10 ms of launch latency on these small graphs).  The whole
     learned V-cycle's time also depends on the hierarchy it builds; that ratio
@@ -174,7 +174,7 @@ def test_trained_model_against_plain(gp, cuda):
                     ("chunglu_50k", graphs.chung_lu(50000, 170000, seed=778))):
         rp, ci = g[0].to(cuda), g[1].to(cuda)
         r = learned.evaluate(model, rp, ci, 32, reps=2)
-        _, st, rep, _ = gp.partition_learned(rp, ci, 32, model, judge=True)
+        _, st, rep, _ = gp.partition_learned(rp, ci, 32, model, fallback=True)
         assert st["cut"] <= r["cut_plain"]
         assert r["ms_gnn"] <= 0.2 * r["ms_plain"] + 10.0, r
         rows.append((name, r["cut_plain"], r["cut_learned"], round(r["cut_ratio"], 4), round(r["time_ratio"], 3)))
@@ -205,5 +205,5 @@ def test_learned_api_rejects_invalid(gp, cuda):
     with pytest.raises(gp.GPError):
         gp.partition_learned(rp, ci, 0, model)
     # still usable
-    p, st, rep, _ = gp.partition_learned(rp, ci, 4, model, judge=True)
+    p, st, rep, _ = gp.partition_learned(rp, ci, 4, model, fallback=True)
     assert st["cut"] == gp.edge_cut(rp, ci, p, 4)[0]

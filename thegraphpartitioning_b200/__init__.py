@@ -372,9 +372,9 @@ def default_gnn() -> GNN:
 
 
 def partition_learned(rowptr, colidx, k: int, model: GNN, imbalance: float = 0.03, seed: int = 0, vwgt=None,
-                      ewgt=None, options=None, judge: bool = True, trace: bool = False, out=None, stream=None):
+                      ewgt=None, options=None, fallback: bool = True, trace: bool = False, out=None, stream=None):
     """V-cycle with the model's scores as matching priorities (torch CUDA
-    tensors).  judge=True also runs the plain V-cycle and keeps the learned
+    tensors).  fallback=True also runs the plain V-cycle and keeps the learned
     partition only when its exact cut <= the plain cut (balance permitting).
     Returns (part, stats, report, trace_events)."""
     import torch
@@ -391,7 +391,7 @@ def partition_learned(rowptr, colidx, k: int, model: GNN, imbalance: float = 0.0
         stream = torch.cuda.current_stream(rowptr.device).cuda_stream
     rc = L.gp_partition_learned_device(n, _ptr(rowptr), _ptr(colidx), _ptr(vwgt), _ptr(ewgt), int(k),
                                        float(imbalance), int(seed) & 0xFFFFFFFFFFFFFFFF, _ptr(part), C.c_void_p(stream),
-                                       C.byref(opt), C.byref(st), model._h, 1 if judge else 0, C.byref(rep), tfn, None)
+                                       C.byref(opt), C.byref(st), model._h, 1 if fallback else 0, C.byref(rep), tfn, None)
     _check(rc)
     return part, st.as_dict(), rep.as_dict(), (col.events if col else [])
 

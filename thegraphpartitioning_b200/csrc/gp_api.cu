@@ -483,7 +483,7 @@ int gp_partition_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_col
 int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx, const int32_t* d_vwgt,
                                 const int32_t* d_ewgt, int32_t k, float imbalance, uint64_t seed, int32_t* d_part_out,
                                 void* stream, const gp_options* opt, gp_stats* stats, const gp_gnn* model,
-                                int32_t judge, gp_learned_report* report, gp_trace_fn trace, void* trace_user) {
+                                int32_t fallback, gp_learned_report* report, gp_trace_fn trace, void* trace_user) {
     return guarded([&] {
         check_args(n, k, imbalance);
         if (!model) throw GpError(GP_EINVAL, "null model");
@@ -513,7 +513,7 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
         rep.cut_learned = sl.cut; rep.max_part_weight_learned = sl.max_part_weight; rep.ms_learned = sl.ms_total;
         rep.ms_gnn = c.ms_gnn;
         rep.kept_learned = 1;
-        if (judge) {
+        if (fallback) {
             // the plain V-cycle into scratch; its result replaces the learned one
             // unless the learned partition is at least as balanced (within the
             // bound) and cuts no more

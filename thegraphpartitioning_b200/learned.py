@@ -171,7 +171,7 @@ def tune_prio_bits(model: GNN, graphs, k: int = 32, candidates=(4, 6, 8, 10, 12,
         for b in candidates:
             model.prio_bits = b
             model.max_level = lv
-            logs = [math.log(max(partition_learned(rp, ci, k, model, judge=False)[1]["cut"], 1) / max(c, 1))
+            logs = [math.log(max(partition_learned(rp, ci, k, model, fallback=False)[1]["cut"], 1) / max(c, 1))
                     for (rp, ci), c in zip(graphs, plain)]
             res[(b, lv)] = math.exp(sum(logs) / len(logs))
             if log:
@@ -186,12 +186,12 @@ def evaluate(model: GNN, rowptr, colidx, k: int, seed: int = 0, imbalance: float
     (one untimed warm-up of each, then the fastest of `reps` runs)."""
     import torch
     partition(rowptr, colidx, k, imbalance=imbalance, seed=seed)
-    partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, judge=False)
+    partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, fallback=False)
     best = None
     for _ in range(reps):
         torch.cuda.synchronize()
         _, sp, _ = partition(rowptr, colidx, k, imbalance=imbalance, seed=seed)
-        _, sl, rep, _ = partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, judge=False)
+        _, sl, rep, _ = partition_learned(rowptr, colidx, k, model, imbalance=imbalance, seed=seed, fallback=False)
         r = {"cut_plain": sp["cut"], "cut_learned": sl["cut"], "imb_plain": sp["imbalance"],
              "imb_learned": sl["imbalance"], "ms_plain": sp["ms_total"], "ms_learned": sl["ms_total"],
              "ms_gnn": rep["ms_gnn"], "balanced_learned": sl["max_part_weight"] <= sl["max_allowed"]}
