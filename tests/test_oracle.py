@@ -162,3 +162,29 @@ def test_rule_helpers(oracle_mod):
     assert bs == sorted(bs) and 0 < min(bs) and max(bs) < 1024
     # edge hash is symmetric in its endpoints
     assert oracle_mod.edge_hash(5, 2, 10, 77) == oracle_mod.edge_hash(5, 2, 77, 10)
+
+
+def test_priority_hook_with_edge_weights_is_plain(oracle_mod):
+    """The learned mode's matching-priority hook, given each level's own edge
+    weights as priorities, must reproduce the plain V-cycle event for event
+    (the priority replaces exactly the edge weight's place in the key)."""
+    from thegraphpartitioning_b200 import graphs
+    from helpers import to_np, weighted
+    from thegraphpartitioning_b200._abi import GP_TR_CONTRACT
+    for g, k, w in ((graphs.rmat(12, seed=4)[:2], 16, False), (graphs.grid2d(40, 45), 5, True)):
+        rp, ci = to_np(*g)
+        ew = vw = None
+        if w:
+            ew, vw = weighted(rp, ci, seed=3)
+        p0, s0, ev0 = oracle_mod.partition(rp, ci, k, 0.03, 6, vwgt=vw, ewgt=ew, trace=True)
+        prio = {0: ew if ew is not None else np.ones(len(ci), np.int32)}
+        for e in ev0:
+            if e["kind"] == GP_TR_CONTRACT:
+                prio[e["level"] + 1] = e["ewgt"]
+        p1, s1, ev1 = oracle_mod.partition(rp, ci, k, 0.03, 6, vwgt=vw, ewgt=ew, trace=True, prio_levels=prio)
+        assert np.array_equal(p0, p1) and s0["cut"] == s1["cut"]
+        assert len(ev0) == len(ev1)
+        for a, b in zip(ev0, ev1):
+            assert a["kind"] == b["kind"] and a["level"] == b["level"] and a["iter"] == b["iter"]
+            if "a0" in a:
+                assert np.array_equal(a["a0"], b["a0"])
