@@ -138,14 +138,7 @@ void build_heavy(Ctx& c, Level& L) {
 __device__ __forceinline__ void argmax_merge(uint64_t& k, int32_t& id, uint64_t k2, int32_t i2) {
     if (k2 > k || (k2 == k && (uint32_t)i2 < (uint32_t)id)) { k = k2; id = i2; }
 }
-__device__ __forceinline__ void warp_argmax(uint64_t& k, int32_t& id) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        uint64_t k2 = __shfl_xor_sync(0xffffffffu, k, o);
-        int32_t i2 = __shfl_xor_sync(0xffffffffu, id, o);
-        argmax_merge(k, id, k2, i2);
-    }
-}
+__device__ __forceinline__ void warp_argmax(uint64_t& k, int32_t& id) { group_argmax64(0xffffffffu, k, id); }
 // block-wide; result valid in thread 0
 __device__ __forceinline__ void block_argmax(uint64_t& k, int32_t& id, uint64_t* sk, int32_t* sid) {
     warp_argmax(k, id);
@@ -243,12 +236,7 @@ __device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
             }
         }
     }
-#pragma unroll
-    for (int o = TILE / 2; o > 0; o >>= 1) {
-        const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
-        const int32_t i2 = __shfl_xor_sync(0xffffffffu, bid, o);
-        argmax_merge(bk, bid, k2, i2);
-    }
+    group_argmax64(TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (lane & ~(TILE - 1))), bk, bid);
     const bool lead = tl == 0;
     if (MODE == 0) {
         if (lead && v >= 0) A.out[v] = valid ? bid : -1;

@@ -71,6 +71,21 @@ __host__ __device__ __forceinline__ uint32_t mag_bucket(uint32_t x) {
     uint32_t mant = (x >> (e - 4)) & 15u;
     return 64u + (uint32_t)(e - 6) * 16u + mant;
 }
+#ifdef __CUDACC__
+// Argmax over the lanes of `mask` (every lane of the group calls it with the
+// group's mask) of (64-bit key, id): the largest key, ties to the smaller id
+// compared unsigned (so -1, "none", loses every tie).  Three redux.sync steps:
+// the key's high half, its low half among the lanes holding the top high
+// half, then the id among the lanes holding the top key.
+__device__ __forceinline__ void group_argmax64(uint32_t mask, uint64_t& k, int32_t& id) {
+    const uint32_t hi = (uint32_t)(k >> 32), lo = (uint32_t)k;
+    const uint32_t mh = __reduce_max_sync(mask, hi);
+    const uint32_t ml = __reduce_max_sync(mask, hi == mh ? lo : 0u);
+    const uint32_t mi = __reduce_min_sync(mask, (hi == mh && lo == ml) ? (uint32_t)id : 0xffffffffu);
+    k = ((uint64_t)mh << 32) | ml;
+    id = (int32_t)mi;
+}
+#endif
 template <class T>
 __device__ __forceinline__ T warp_incl_scan(T x) {
     const int lane = threadIdx.x & 31;

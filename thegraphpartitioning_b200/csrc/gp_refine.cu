@@ -36,19 +36,25 @@ enum { MODE_LP = 0, MODE_RB = 1, MODE_EVAL = 2 };
 __device__ __forceinline__ void argmax_q(uint64_t& bk, int32_t& bq, uint64_t k2, int32_t q2) {
     if (k2 > bk || (k2 == bk && (uint32_t)q2 < (uint32_t)bq)) { bk = k2; bq = q2; }
 }
-__device__ __forceinline__ void warp_argmax_q(uint64_t& bk, int32_t& bq) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
-        int32_t q2 = __shfl_xor_sync(0xffffffffu, bq, o);
-        argmax_q(bk, bq, k2, q2);
-    }
-}
+__device__ __forceinline__ void warp_argmax_q(uint64_t& bk, int32_t& bq) { group_argmax64(0xffffffffu, bk, bq); }
 template <class T>
 __device__ __forceinline__ T warp_sum(T x) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
+}
+
+// Argmax over a lane group of (connectivity h > 0, part q): largest h, ties
+// to the smaller q; h = 0 means "no candidate" and yields (0, -1).  Two
+// redux.sync steps replace the shuffle tree (connectivities fit in 32 bits).
+__device__ __forceinline__ void group_argmax_u32(uint32_t mask, uint64_t& bk, int32_t& bq, uint32_t h, int32_t q) {
+    const uint32_t mh = __reduce_max_sync(mask, h);
+    const uint32_t mq = __reduce_min_sync(mask, (h != 0u && h == mh) ? (uint32_t)q : 0xffffffffu);
+    bk = mh;
+    bq = mh ? (int32_t)mq : -1;
+}
+__device__ __forceinline__ void argmax_u32(uint32_t& bh, int32_t& bq, uint32_t h, int32_t q) {
+    if (h > bh || (h == bh && (uint32_t)q < (uint32_t)bq)) { bh = h; bq = q; }
 }
 
 // LP candidate rule: gain >= 0, or -gain < own/den
@@ -152,25 +158,16 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
     if (has) { q = A.part[__ldcs(&A.g.ci[e])]; w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
-    int32_t cross = (has && q != p) ? w : 0, tot = w;
-#pragma unroll
-    for (int o = TILE / 2; o > 0; o >>= 1) {
-        cross += __shfl_xor_sync(0xffffffffu, cross, o);
-        tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    }
+    const uint32_t tmask = TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (tix * TILE));
+    const int32_t cross = (int32_t)__reduce_add_sync(tmask, (has && q != p) ? (uint32_t)w : 0u);
+    const int32_t tot = (int32_t)__reduce_add_sync(tmask, (uint32_t)w);
     const uint32_t key = has ? (((uint32_t)tix << 20) | (uint32_t)q) : (0x80000000u | (uint32_t)lane);
     const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    const int32_t connq = (int32_t)__reduce_add_sync(peers, (uint32_t)w);
+    const uint32_t connq = __reduce_add_sync(peers, (uint32_t)w);
     const bool lead = has && lane == __ffs(peers) - 1;
-    uint64_t bk = 0;
-    int32_t bq = -1;
-    if (active && lead && q != p && (mode != MODE_RB || !over[q])) { bk = (uint64_t)connq; bq = q; }
-#pragma unroll
-    for (int o = TILE / 2; o > 0; o >>= 1) {
-        const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bk, o);
-        const int32_t q2 = __shfl_xor_sync(0xffffffffu, bq, o);
-        argmax_q(bk, bq, k2, q2);
-    }
+    uint64_t bk;
+    int32_t bq;
+    group_argmax_u32(tmask, bk, bq, (active && lead && q != p && (mode != MODE_RB || !over[q])) ? connq : 0u, q);
     bool take = false;
     if (tl == 0 && v >= 0) {
         acc += cross;
@@ -181,10 +178,13 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
 }
 
 // bucket 2: one row per warp, shared-memory histogram.  The row is swept
-// 128 entries at a time (4 independent loads per lane in flight).  For rows
-// at least as long as k the best part is taken over the k histogram bins,
+// 128 entries at a time (4 independent loads per lane in flight).  The own
+// part is never added (its connectivity is tot - cross), which keeps the
+// most contended bin out of the shared-memory atomics.  For rows at least as
+// long as k, or k <= kBinsK, the best part is taken over the k histogram bins,
 // otherwise over the row's entries again (same candidates: parts with a
 // non-zero connection).
+constexpr int kBinsK = 256;
 __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
                                           int32_t* hist, int64_t& acc) {
     const int lane = threadIdx.x & 31;
@@ -206,29 +206,31 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
         for (int c = 0; c < 4; ++c) {
             tot += w[c];
             if (q[c] >= 0 && q[c] != p) cross += w[c];
-            if (active) hist_add(hist, q[c], w[c], q[c] >= 0);
+            if (active) hist_add(hist, q[c], w[c], q[c] >= 0 && q[c] != p);
         }
     }
-    cross = warp_sum(cross);
-    tot = warp_sum(tot);
+    cross = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)cross);
+    tot = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)tot);
     uint64_t bk = 0;
     int32_t bq = -1;
     if (active) {
         __syncwarp();
-        if (end - beg >= A.k) {
+        uint32_t lh = 0;
+        int32_t lq = -1;
+        if (end - beg >= A.k || A.k <= kBinsK) {
             for (int q = lane; q < A.k; q += 32) {
                 const int32_t h = hist[q];
-                if (h > 0 && q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)h, q);
+                if (h > 0 && q != p && (mode != MODE_RB || !over[q])) argmax_u32(lh, lq, (uint32_t)h, q);
             }
-            warp_argmax_q(bk, bq);
+            group_argmax_u32(0xffffffffu, bk, bq, lh, lq);
             __syncwarp();
             for (int q = lane; q < A.k; q += 32) hist[q] = 0;
         } else {
             for (int64_t e = beg + lane; e < end; e += 32) {
                 const int32_t q = A.part[__ldcs(&A.g.ci[e])];
-                if (q != p && (mode != MODE_RB || !over[q])) argmax_q(bk, bq, (uint64_t)hist[q], q);
+                if (q != p && (mode != MODE_RB || !over[q])) argmax_u32(lh, lq, (uint32_t)hist[q], q);
             }
-            warp_argmax_q(bk, bq);
+            group_argmax_u32(0xffffffffu, bk, bq, lh, lq);
             __syncwarp();
             for (int64_t e = beg + lane; e < end; e += 32) hist[A.part[__ldcs(&A.g.ci[e])]] = 0;
         }
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
             for (int c = 0; c < 4; ++c) {
                 tot += ww[c];
                 if (qq[c] >= 0 && qq[c] != p) cross += ww[c];
-                if (active) hist_add(hist, qq[c], ww[c], qq[c] >= 0);
+                if (active) hist_add(hist, qq[c], ww[c], qq[c] >= 0 && qq[c] != p);
             }
         }
         cross = warp_sum(cross); tot = warp_sum(tot);
