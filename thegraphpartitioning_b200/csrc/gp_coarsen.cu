@@ -246,7 +246,7 @@ __device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256) k_match_scan(MatchArgs A) {
+__global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
     __shared__ uint64_t sk[32];
     __shared__ int32_t sid[32];
     const int lane = threadIdx.x & 31;
