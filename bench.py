@@ -121,6 +121,50 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+# clock reasons that void a timed run (sw_power_cap is kept and reported)
+REJECT_REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown")
+
+
+def clock_rejections(summary):
+    """Why a timed run's clock record voids it: a slowdown reason, or SM clocks
+    well below their maximum with no reason that explains it (a leftover lock)."""
+    reasons = summary.get("reasons") or []
+    out = [r for r in reasons if r in REJECT_REASONS]
+    sm, smax = summary.get("sm_mhz"), summary.get("sm_max_mhz")
+    explained = [r for r in reasons if r != "applications_clocks_setting"]
+    if sm and smax and sm < 0.8 * smax and not explained:
+        out.append("sm_clock_low_without_reason")
+    return out
+
+
+def timed_region(region, index, dist=None, dev=None):
+    """region() runs the timed steps and returns (ms, payload).  It runs under
+    the clock sampler; a run that clock_rejections() voids (on any rank) is
+    measured once more on every rank, and the first run's reasons are kept in
+    the summary under "rejected_first_run"."""
+    import torch
+    with ClockSampler(index) as clocks:
+        t_ms, payload = region()
+    summ = clocks.summary()
+    bad = clock_rejections(summ)
+    flag = 1.0 if bad else 0.0
+    if dist:
+        tt = torch.tensor([flag], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        flag = float(tt.item())
+    if flag > 0:
+        first = {"reasons": bad or ["another rank"], "sm_mhz": summ["sm_mhz"]}
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(index) as clocks:
+            t_ms, payload = region()
+        summ = clocks.summary()
+        summ["rejected_first_run"] = first
+    return t_ms, payload, summ
+
+
 def measured_hbm_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -288,16 +332,17 @@ def run_batch(args, rank, world, dev, dist):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    stats = None
-    with ClockSampler(dev.index or 0) as clocks:
+    def region():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        st = None
         e0.record(stream)
         for _ in range(args.steps):
-            _, stats = gp.partition_batch(gs, ks, args.imbalance, seeds, options=opts, workers=args.workers, outs=outs)
+            _, st = gp.partition_batch(gs, ks, args.imbalance, seeds, options=opts, workers=args.workers, outs=outs)
         e1.record(stream)
         torch.cuda.synchronize()
-    t_ms = e0.elapsed_time(e1)
+        return e0.elapsed_time(e1), st
+    t_ms, stats, clock_summary = timed_region(region, dev.index or 0, dist, dev)
     # end to end: pinned host CSR in, part arrays out, through the same call
     hs = [(g[0].cpu().pin_memory(), g[1].cpu().pin_memory()) for g in gs]
     hout = [torch.empty(o.numel(), dtype=torch.int32).pin_memory() for o in outs]
@@ -343,7 +388,7 @@ def run_batch(args, rank, world, dev, dist):
                     "h2d_bytes_per_step": int(8 * (n_all + args.batch_count) + 8 * m_all),
                     "d2h_bytes_per_step": int(4 * n_all), "ms_per_step": 1e3 * t_e2e},
             "gpu_launches": int(launches * args.steps),   # launches of one batch call x timed calls
-            "clocks": clocks.summary(),
+            "clocks": clock_summary,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -396,17 +441,18 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    stats = []
-    with ClockSampler(local) as clocks:
+    def region():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        sts = []
         e0.record(stream)
         for _ in range(args.steps):
             _, st, _ = gp.partition(rp, ci, args.k, args.imbalance, args.seed, options=opts, out=part)
-            stats.append(st)
+            sts.append(st)
         e1.record(stream)
         torch.cuda.synchronize()
-    t_ms = e0.elapsed_time(e1)
+        return e0.elapsed_time(e1), sts
+    t_ms, stats, clock_summary = timed_region(region, local, dist, dev)
     if dist:
         tt = torch.tensor([t_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -478,7 +524,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": 8 * (n + 1) + 4 * 2 * m,
                     "d2h_bytes_per_step": 4 * n, "ms_per_step": 1e3 * t_e2e / args.e2e_steps},
             "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
-            "clocks": clocks.summary(),
+            "clocks": clock_summary,
         }
         if world == 1 and not args.no_cpu_baseline:
             line.update(cpu_sample(args))
