@@ -90,3 +90,47 @@ def test_timed_region_remeasures_once(bench, monkeypatch):
     _FakeSampler.queue = [dict(hot), dict(hot)]
     t, payload, s = bench.timed_region(region, 0)
     assert len(calls) == 2 and s["reasons"] == ["hw_thermal_slowdown"]
+
+
+def _rank_remeasure(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    import torch
+    torch.cuda.synchronize = lambda *a, **k: None
+    good = {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 5}
+    hot = {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["hw_slowdown"], "samples": 5}
+    # only rank 1 sees a slowdown in its first run
+    _FakeSampler.queue = [dict(hot if rank == 1 else good), dict(good)]
+    bench.ClockSampler = _FakeSampler
+    calls = []
+
+    def region():
+        calls.append(1)
+        dist.barrier()   # a collective inside the timed region, as the bench's ranks have
+        return 1.0, None
+
+    _, _, s = bench.timed_region(region, 0, dist, None)
+    out[rank] = (len(calls), s.get("rejected_first_run", {}).get("reasons"))
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_remeasure_together():
+    """A voided run on one rank makes every rank time the region again, so
+    all ranks take the same collective steps."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = 30500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank_remeasure, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0] == (2, ["another rank"])
+    assert out[1] == (2, ["hw_slowdown"])
