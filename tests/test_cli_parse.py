@@ -71,3 +71,29 @@ def test_parse_errors(tmp_path):
         f.write(" ".join(map(str, ci[:10].tolist())) + " x7 " + " ".join(map(str, ci[11:].tolist())))
     r = _run([d, "100", "500", "4"], str(tmp_path))
     assert r.returncode == 2 and "not an integer at element 10" in r.stderr
+
+
+def test_preprocess_output_feeds_the_cli(tmp_path):
+    """Ranks 3-4 of the pipeline together: an edge list turned into row.txt /
+    column.txt / weight.txt by the preprocessing restatement is read back by
+    the CLI exactly, in both command lines (the reference's users run
+    conversion.py and then gpu_part on its output)."""
+    from thegraphpartitioning_b200 import preprocess
+    rng = np.random.default_rng(5)
+    src = rng.integers(0, 3000, size=20000)
+    dst = rng.integers(0, 3000, size=20000)
+    edges = str(tmp_path / "g.tsv")
+    with open(edges, "w") as f:
+        for a, b in zip(src.tolist(), dst.tolist()):
+            f.write(f"{a}\t{b}\t1\n")
+    out = str(tmp_path / "csr")
+    assert preprocess.main([edges, out]) == 0
+    rp, ci = preprocess.to_csr(src, dst)
+    rp = rp.astype(np.int64); ci = ci.astype(np.int64)
+    n, m = len(rp) - 1, len(ci)
+    r = _run([out, str(n), str(m), "8"], str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert f"n={n} m={m} weights=1 checksum={fnv(rp, ci, np.ones(m, dtype=np.int64))}" in r.stdout
+    r = _run([os.path.join(out, "row.txt"), os.path.join(out, "column.txt"), "8"], str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert f"n={n} m={m} weights=1" in r.stdout   # weight.txt beside row.txt is picked up
