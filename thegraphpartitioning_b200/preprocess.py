@@ -48,8 +48,9 @@ def load_edges(path: str):
 def to_csr(src, dst):
     """Symmetric CSR without self-loops, duplicates or isolated vertices
     (renumbered in id order).  Returns (rowptr int64, colidx int32)."""
-    s = torch.as_tensor(np.asarray(src), dtype=torch.int64)
-    d = torch.as_tensor(np.asarray(dst), dtype=torch.int64)
+    # own writable copies: readers (pandas, mmread) may hand out read-only arrays
+    s = torch.from_numpy(np.array(src, dtype=np.int64))
+    d = torch.from_numpy(np.array(dst, dtype=np.int64))
     n = int(max(int(s.max()), int(d.max())) + 1) if s.numel() else 0
     rowptr, colidx, _ = csr_from_edges(s, d, n, drop_isolated=True)
     return rowptr.numpy(), colidx.numpy()
