@@ -35,7 +35,11 @@ def load_edges(path: str):
     ext = os.path.splitext(path)[1]
     if ext in (".mtx", ".mmio"):
         from scipy.io import mmread
-        coo = mmread(path).tocoo()
+        try:
+            mat = mmread(path, spmatrix=False)   # sparse array (newer scipy)
+        except TypeError:
+            mat = mmread(path)
+        coo = mat.tocoo()
         return np.asarray(coo.col, dtype=np.int64), np.asarray(coo.row, dtype=np.int64)
     skip = {".tsv": 0, ".txt": 4, ".tsv_1": 1}
     if ext not in skip:
