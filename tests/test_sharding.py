@@ -46,3 +46,18 @@ def test_two_gloo_ranks_agree_on_shards():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert out[0] == 1 and out[1] == 1
+
+
+def test_autotune_sample_keeps_size_mix():
+    """The tuner's sample: distinct indices, every step-th graph of the batch in
+    decreasing cost order, so large and small graphs are both represented."""
+    from thegraphpartitioning_b200.autotune import _sample
+    costs = [(i * 7919) % 1000 + 1 for i in range(1000)]
+    idx = _sample(len(costs), costs, 100)
+    assert len(idx) == 100 and len(set(idx)) == 100
+    order = sorted(range(1000), key=lambda i: (-costs[i], i))
+    assert idx[0] == order[0]                      # the largest graph is in
+    assert [costs[i] for i in idx] == sorted((costs[i] for i in idx), reverse=True)
+    ranks = [order.index(i) for i in idx]
+    assert max(ranks) >= 900                       # and the small end too
+    assert _sample(5, [3, 1, 2, 5, 4], 10) == [3, 4, 0, 2, 1]   # sample larger than the batch: all, by cost
