@@ -29,7 +29,7 @@ def test_clock_rejections(bench):
         ["sm_clock_low_without_reason"]
     assert bench.clock_rejections({"sm_mhz": 1000.0, "sm_max_mhz": 1965.0,
                                    "reasons": ["applications_clocks_setting"]}) == ["sm_clock_low_without_reason"]
-    # no samples (no nvidia-smi): nothing to judge
+    # no samples (no nvidia-smi): nothing to go by
     assert bench.clock_rejections({"sm_mhz": None, "sm_max_mhz": None, "reasons": []}) == []
 
 
