@@ -270,7 +270,8 @@ def run_reference(args, rank):
                    "seed": args.seed, "timed_sample": sample, "cut": min(cuts), "copies_agree": len(cuts) == 1},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's path runs only on a GPU with an external gpmetis; its CPU counterpart "
+        "note": "the reference's path runs only on a GPU with an external gpmetis, and is not run on the shared "
+                "GPUs (its move sort can write destCounts[-1], src/gpu_part.cu:378/493); its CPU counterpart "
                 "here is the oracle (sequential restatement of the same deterministic rules), one copy per core",
     }
     print(json.dumps(line), flush=True)
