@@ -2,7 +2,7 @@
 
 The reference ships no tests or golden vectors (its only worked example is the
 5-vertex CSR preview in README.md), so the oracle is pinned by known answers:
-paths (optimum k-1), disjoint cliques (0), two cliques joined by one edge (1),
+paths (optimum k-1), rings (optimum k), disjoint cliques (0), two cliques joined by one edge (1),
 grids (optimum min(R, C) for a bisection), plus exact invariants on every run.
 """
 import numpy as np
@@ -32,6 +32,24 @@ def test_path_optimum(oracle_mod, n, k):
     cut, pw = _check_result(oracle_mod, rp, ci, part, st, k)
     assert cut == k - 1
     assert pw.max() <= st["max_allowed"]
+
+
+def _ring(n):
+    rows = [sorted({(v - 1) % n, (v + 1) % n}) for v in range(n)]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int64)
+    return rp, np.array([u for r in rows for u in r], dtype=np.int32)
+
+
+@pytest.mark.parametrize("n,k,slack", [(100, 4, 0), (999, 7, 0), (1000, 8, 0), (4096, 64, 2)])
+def test_ring_optimum(oracle_mod, n, k, slack):
+    """A cycle cut into k arcs has the optimal cut k; small k reach it exactly
+    on every seed, k = 64 on 4096 vertices within two extra edges."""
+    rp, ci = _ring(n)
+    for seed in range(3):
+        part, st, _ = oracle_mod.partition(rp, ci, k, 0.03, seed=seed)
+        cut, pw = _check_result(oracle_mod, rp, ci, part, st, k)
+        assert k <= cut <= k + slack
+        assert pw.max() <= st["max_allowed"]
 
 
 @pytest.mark.parametrize("count,size", [(8, 20), (4, 50), (16, 12)])
