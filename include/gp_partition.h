@@ -61,7 +61,7 @@ typedef struct gp_options {
     int32_t two_hop;            /* >0 or 0: pair leftovers sharing an anchor; <0: off   */
     int32_t init_trials;        /* initial-partition trials (default 64)                */
     int32_t refine_max_iters;   /* max refinement iterations per level (default 64)     */
-    int32_t refine_patience;    /* stop after this many non-improving iterations (12)   */
+    int32_t refine_patience;    /* stop after this many non-improving iterations (4)    */
     int32_t lp_filter_den;      /* negative-gain filter: -gain < conn_own/den (4)      */
     int32_t strong_after;       /* consecutive rebalance iterations before strong (2)  */
     int32_t check_input;        /* 0/1: structural checks, 2: +symmetry, <0: none        */

@@ -110,7 +110,7 @@ void resolve_options(const gp_options* in, int64_t n, int32_t k, gp_options* o) 
     if (d.two_hop == 0) d.two_hop = 1;          // <0: off
     if (d.init_trials <= 0) d.init_trials = 64;
     if (d.refine_max_iters <= 0) d.refine_max_iters = 64;
-    if (d.refine_patience <= 0) d.refine_patience = 12;
+    if (d.refine_patience <= 0) d.refine_patience = 4;
     if (d.lp_filter_den <= 0) d.lp_filter_den = 4;
     if (d.strong_after <= 0) d.strong_after = 2;
     if (d.check_input == 0) d.check_input = 1;  // <0: no structural checks
