@@ -40,6 +40,11 @@ def _cases():
     yield "chunglu_k8_mixed", graphs.chung_lu(12000, 40000, seed=2), 8, 0.03, None, {"small_level_n": 3000}
     yield "er_k64_cta", graphs.erdos_renyi(16000, 8.0, seed=8), 64, 0.03, None, {"small_level_n": 16384}
     yield "rmat12_k16_ctas2", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"ctas_per_sm": 2}
+    # a longer refinement patience (more label-propagation / rebalancing cycles per level),
+    # in the multi-kernel loop and in the one-block level loop
+    yield "rmat12_k16_patience12", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"refine_patience": 12}
+    yield "er_k64_cta_patience12", graphs.erdos_renyi(16000, 8.0, seed=8), 64, 0.03, None, \
+        {"small_level_n": 16384, "refine_patience": 12}
     # many parts: histograms of k bins, rebalancing over hundreds of parts
     yield "chunglu_k512", graphs.chung_lu(20000, 70000, seed=12), 512, 0.03, None, {}
     yield "grid120_k1000_w", graphs.grid2d(120, 120), 1000, 0.05, "w", {}
