@@ -57,7 +57,7 @@ extern "C" {
 typedef struct gp_options {
     int32_t version;            /* GP_OPTIONS_VERSION                                   */
     int32_t coarsen_to;         /* stop coarsening at <= this many vertices (0: auto)   */
-    int32_t match_rounds;       /* max handshake rounds per level (default 8)           */
+    int32_t match_rounds;       /* max handshake rounds per level (default 4)           */
     int32_t two_hop;            /* >0 or 0: pair leftovers sharing an anchor; <0: off   */
     int32_t init_trials;        /* initial-partition trials (default 64)                */
     int32_t refine_max_iters;   /* max refinement iterations per level (default 64)     */
@@ -256,9 +256,10 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
 
 /* No counterpart in the reference (which has no library API).
  * Same result as gp_edge_cut_device, for callers that must not allocate:
- * code running while a CUDA graph is captured on its stream, code inside an
- * allocator or memory-pool callback, loops that forbid allocation after
- * start-up, processes whose device memory another framework has reserved.
+ * code inside an allocator or memory-pool callback (an allocation there
+ * re-enters the allocator), loops that forbid allocation after start-up
+ * (an allocation can block or fail mid-loop), processes whose device memory
+ * another framework has reserved (nothing is left to allocate).
  * gp_edge_cut_device may grow a cached workspace with cudaMalloc on first use;
  * this variant calls no cudaMalloc, cudaFree or other allocating routine.  Its
  * scratch is a fixed array in device memory (about 8 KB, held by every device

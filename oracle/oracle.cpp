@@ -55,10 +55,20 @@ inline uint64_t mix64(uint64_t x) {
 inline uint64_t level_salt(uint64_t seed, int level) {
     return mix64(seed ^ mix64(0x9E3779B97F4A7C15ULL * (uint64_t)(level + 1)));
 }
-// Symmetric per-edge tie-break hash: both endpoints see the same value.
-inline uint32_t edge_hash(uint64_t salt, int32_t a, int32_t b) {
+// MurmurHash3's 32-bit finalizer (Appleby; its published constants).
+inline uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu;
+    h ^= h >> 13; h *= 0xC2B2AE35u;
+    h ^= h >> 16; return h;
+}
+// The matching tie-break of a level is salted with the level salt's high half.
+inline uint32_t edge_salt(uint64_t seed, int level) { return (uint32_t)(level_salt(seed, level) >> 32); }
+// Symmetric per-edge tie-break hash: both endpoints see the same value.  The
+// ordered ids are spread by two odd constants (the 32-bit golden ratio and
+// xxHash's PRIME32_2), summed with the salt modulo 2^32 and finalized.
+inline uint32_t edge_hash(uint32_t salt, int32_t a, int32_t b) {
     uint32_t lo = (uint32_t)std::min(a, b), hi = (uint32_t)std::max(a, b);
-    return (uint32_t)(mix64(salt ^ (((uint64_t)lo << 32) | hi)) >> 32);
+    return fmix32(lo * 0x9E3779B1u + hi * 0x85EBCA77u + salt);
 }
 // Matching priority of an edge: heavier first, then the hash.
 inline uint64_t edge_key(int32_t w, uint32_t h) { return ((uint64_t)(uint32_t)w << 32) | h; }
@@ -106,7 +116,7 @@ void resolve_options(const gp_options* in, int64_t n, int32_t k, gp_options* o) 
     if (in) d = *in;
     d.version = GP_OPTIONS_VERSION;
     if (d.coarsen_to <= 0) d.coarsen_to = (int32_t)std::max<int64_t>(1024, 32LL * k);
-    if (d.match_rounds <= 0) d.match_rounds = 8;
+    if (d.match_rounds <= 0) d.match_rounds = 4;
     if (d.two_hop == 0) d.two_hop = 1;          // <0: off
     if (d.init_trials <= 0) d.init_trials = 64;
     if (d.refine_max_iters <= 0) d.refine_max_iters = 64;
@@ -165,7 +175,7 @@ int64_t max_of(const std::vector<int64_t>& a) {
 // are paired in id order within each anchor group (two-hop pairing).
 std::vector<int32_t> match_level(const Graph& g, int level, const Params& P, int* rounds_out, int64_t* pairs_out) {
     const int64_t n = g.n;
-    const uint64_t salt = level_salt(P.seed, level);
+    const uint32_t salt = edge_salt(P.seed, level);
     const int32_t* pr = P.prio ? P.prio(P.prio_user, level, g.m()) : nullptr;
     const int32_t* key_w = pr ? pr : g.ew.data();   // high word of the matching priority
     std::vector<int32_t> match(n, -1), prop(n, -1);
@@ -780,7 +790,7 @@ int gpo_edge_cut(int64_t n, const int64_t* rowptr, const int32_t* colidx, const 
 
 // Exposed pieces of the rule set, for unit tests of the hash and bucket.
 uint64_t gpo_mix64(uint64_t x) { return mix64(x); }
-uint32_t gpo_edge_hash(uint64_t seed, int32_t level, int32_t a, int32_t b) { return edge_hash(level_salt(seed, level), a, b); }
+uint32_t gpo_edge_hash(uint64_t seed, int32_t level, int32_t a, int32_t b) { return edge_hash(edge_salt(seed, level), a, b); }
 uint32_t gpo_loss_bucket(int32_t loss) { return loss_bucket(loss); }
 
 }  // extern "C"

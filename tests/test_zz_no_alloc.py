@@ -1,10 +1,13 @@
-"""The allocation-free edge-cut entry point, checked against the regular one.
+"""The allocation-free edge-cut entry point, checked against the regular one
+and against the oracle.
 
-gp_edge_cut_device_noalloc serves callers that cannot allocate device memory
-(stream capture in progress, allocator callbacks, allocation-free loops, fully
-reserved devices): its scratch is a fixed device array shared by every call.
-This file is collected last so that a run stopping at the first failure has
-run every other test first; it passes alone and after the rest of the suite.
+gp_edge_cut_device_noalloc serves callers that cannot allocate device memory:
+code inside an allocator or memory-pool callback (an allocation would
+re-enter the allocator), allocation-free serving loops (an allocation can
+block or fail mid-loop) and devices whose memory another framework has
+reserved.  Its scratch is a fixed device array shared by every call.  This
+file is collected last so that a run stopping at the first failure has run
+every other test first; it passes alone and after the rest of the suite.
 """
 import ctypes as C
 
@@ -37,31 +40,53 @@ def _noalloc(f, rp, ci, ew, vw, part, k):
     return rc, int(cut.value), pw
 
 
-def test_noalloc_matches_regular_entry_point_twice(gp, cuda):
+def _device_free_bytes():
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info()[0]
+
+
+def test_noalloc_matches_regular_entry_point_twice(gp, cuda, oracle_mod):
     lib, f = _bind(gp)
     rp, ci = to_np(*graphs.chung_lu(40000, 150000, seed=7))
     ew, vw = weighted(rp, ci, seed=3)
     d = lambda a: torch.from_numpy(a).to(cuda)
     drp, dci, dew, dvw = d(rp), d(ci), d(ew), d(vw)
     n = len(rp) - 1
-    # two calls in a row with different partitions and k: the second must not
-    # see the first call's accumulators
+    # two partitions with different k: the second call must not see the first
+    # call's accumulators
+    cases = []
     for k, mult in ((13, 7919), (64, 104729)):
-        part = d((np.arange(n) * mult % k).astype(np.int32))
+        hpart = (np.arange(n) * mult % k).astype(np.int32)
+        cut_ref, pw_ref = gp.edge_cut(drp, dci, d(hpart), k, ewgt=dew, vwgt=dvw)
+        cut_or, pw_or = oracle_mod.edge_cut(rp, ci, hpart, k, ewgt=ew, vwgt=vw)
+        assert cut_ref == cut_or and np.array_equal(pw_ref, pw_or)
+        cases.append((k, d(hpart), cut_or, pw_or))
+    # first call on this device: looks up the scratch array's address and
+    # loads the kernels
+    assert _noalloc(f, drp, dci, dew, dvw, cases[0][1], cases[0][0])[0] == 0, lib.gp_last_error().decode()
+    # without the library's cached workspace, two calls in a row take no
+    # device memory
+    gp.release_workspace()
+    free0 = _device_free_bytes()
+    for k, part, cut_or, pw_or in cases:
         rc, cut, pw = _noalloc(f, drp, dci, dew, dvw, part, k)
         assert rc == 0, lib.gp_last_error().decode()
-        cut_ref, pw_ref = gp.edge_cut(drp, dci, part, k, ewgt=dew, vwgt=dvw)
-        assert cut == cut_ref
-        assert np.array_equal(pw, pw_ref)
+        assert cut == cut_or
+        assert np.array_equal(pw, pw_or)
+    free1 = _device_free_bytes()
+    assert free1 >= free0 - (1 << 20), (free0, free1)
 
 
-def test_noalloc_unit_weights_and_limits(gp, cuda):
+def test_noalloc_unit_weights_and_limits(gp, cuda, oracle_mod):
     lib, f = _bind(gp)
     rp, ci = graphs.grid2d(200, 300)
+    hpart = (np.arange(rp.numel() - 1) % 4).astype(np.int32)
+    cut_or, pw_or = oracle_mod.edge_cut(rp.numpy(), ci.numpy(), hpart, 4)
     rp, ci = rp.to(cuda), ci.to(cuda)
-    part = (torch.arange(rp.numel() - 1, device=cuda) % 4).to(torch.int32)
+    part = torch.from_numpy(hpart).to(cuda)
     rc, cut, pw = _noalloc(f, rp, ci, None, None, part, 4)
     assert rc == 0
+    assert cut == cut_or and np.array_equal(pw, pw_or)
     assert (cut, list(pw)) == (lambda r: (r[0], list(r[1])))(gp.edge_cut(rp, ci, part, 4))
     rc, _, _ = _noalloc(f, rp, ci, None, None, part, 1025)   # beyond the scratch
     assert rc == -1 and "GP_NOALLOC_MAX_K" in lib.gp_last_error().decode()

@@ -176,7 +176,7 @@ struct MatchArgs {
     int64_t nlist[3];
     const int32_t* match;
     int32_t* out;             // MODE 0: proposals
-    uint64_t salt;
+    uint32_t salt;
     int64_t maxvw;
     uint64_t* keys;           // MODE 1: (anchor << nbits | v)
     int64_t* nkeys;
@@ -418,7 +418,7 @@ __global__ void k_max_vw(int64_t n, const int32_t* __restrict__ vw, int64_t* __r
 int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t* match, int* rounds_out,
                     const int32_t* prio) {
     const DGraph& g = L.g;
-    const uint64_t salt = level_salt(P.seed, level);
+    const uint32_t salt = edge_salt(P.seed, level);
     auto mk = c.tmp->save();
     int32_t* prop = c.tmp_alloc<int32_t>(g.n);
     int32_t* wl[2][3];

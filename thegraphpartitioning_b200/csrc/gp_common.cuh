@@ -54,9 +54,22 @@ __host__ __device__ __forceinline__ uint64_t trial_salt(uint64_t seed, int t) {
 __host__ __device__ __forceinline__ uint64_t depth_salt(uint64_t tsalt, int d) {
     return mix64(tsalt ^ mix64(0x8CB92BA72F3D8DD7ULL * (uint64_t)(d + 1)));
 }
-__host__ __device__ __forceinline__ uint32_t edge_hash(uint64_t salt, int32_t a, int32_t b) {
-    uint32_t lo = (uint32_t)(a < b ? a : b), hi = (uint32_t)(a < b ? b : a);
-    return (uint32_t)(mix64(salt ^ (((uint64_t)lo << 32) | hi)) >> 32);
+// MurmurHash3's 32-bit finalizer (Appleby, published constants)
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu;
+    h ^= h >> 13; h *= 0xC2B2AE35u;
+    h ^= h >> 16; return h;
+}
+// 32-bit salt of a level's matching tie-break (high half of the level salt)
+__host__ __device__ __forceinline__ uint32_t edge_salt(uint64_t seed, int level) {
+    return (uint32_t)(level_salt(seed, level) >> 32);
+}
+// Symmetric per-edge tie-break: the two ids, ordered, times two odd constants
+// (golden ratio, xxHash's second prime) plus the salt, then fmix32.  All
+// 32-bit: two IMADs and the finalizer per entry of every matching round.
+__host__ __device__ __forceinline__ uint32_t edge_hash(uint32_t salt, int32_t a, int32_t b) {
+    const uint32_t lo = (uint32_t)(a < b ? a : b), hi = (uint32_t)(a < b ? b : a);
+    return fmix32(lo * 0x9E3779B1u + hi * 0x85EBCA77u + salt);
 }
 __host__ __device__ __forceinline__ uint64_t edge_key(int32_t w, uint32_t h) {
     return ((uint64_t)(uint32_t)w << 32) | h;

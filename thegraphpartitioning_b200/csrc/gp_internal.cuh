@@ -61,7 +61,7 @@ inline void resolve_options(const gp_options* in, int32_t k, gp_options* o) {
     if (in) d = *in;
     d.version = GP_OPTIONS_VERSION;
     if (d.coarsen_to <= 0) d.coarsen_to = (int32_t)std::max<int64_t>(1024, 32LL * k);
-    if (d.match_rounds <= 0) d.match_rounds = 8;
+    if (d.match_rounds <= 0) d.match_rounds = 4;
     if (d.two_hop == 0) d.two_hop = 1;
     if (d.init_trials <= 0) d.init_trials = 64;
     if (d.refine_max_iters <= 0) d.refine_max_iters = 64;

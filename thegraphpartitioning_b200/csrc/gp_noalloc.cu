@@ -3,10 +3,10 @@
 // gp_edge_cut_device() takes its scratch (the cut accumulator, the k part
 // weight accumulators and a validation word) from the library's device
 // workspace, which grows with cudaMalloc on first use.  Some callers cannot
-// allow that: code running while a CUDA graph is being captured on their
-// stream, code inside a custom allocator or memory-pool callback, real-time
-// loops that forbid allocation after start-up, and hosts whose device memory
-// is fully reserved by another framework.  gp_edge_cut_device_noalloc() is the
+// allow that: code inside a custom allocator or memory-pool callback (an
+// allocation would re-enter the allocator), real-time loops that forbid
+// allocation after start-up (an allocation can block or fail mid-loop), and
+// hosts whose device memory is fully reserved by another framework.  gp_edge_cut_device_noalloc() is the
 // same computation with its scratch in a fixed file-scope __device__ array.
 //
 // Limits and behaviour:
