@@ -19,8 +19,11 @@ the oracle, so this script runs it once on the CPU and records:
           src/gpu_part.cu:857).
 
 bench.py compares its timed partition against the oracle record and reports
-the METIS record beside its own cut and time.  Run (about 15 minutes on one
-core, about 30 GB of host memory at its peak):
+the METIS record beside its own cut and time.  The oracle takes about 13
+minutes on one core; METIS keeps every level of its hierarchy in 64-bit
+arrays and needs more than 60 GB of host memory on this graph, so the two
+records can be made in separate runs on different hosts (each run keeps the
+records already in the output file):
 
     python tests/golden/make_full_fixtures.py [--skip-oracle] [--skip-metis]
 """
@@ -75,6 +78,13 @@ def main():
                     "m_undirected": m, "sha256_rowptr_colidx": sha256_of(rp, ci)}
     rec["args"] = {"k": args.k, "imbalance": args.imbalance, "seed": args.seed}
     W = n
+
+    def save():
+        with open(args.out, "w") as f:
+            json.dump(rec, f, indent=1)
+            f.write("\n")
+
+    save()
     if not args.skip_oracle:
         t = time.perf_counter()
         part, st, _ = oracle.partition(rp, ci, args.k, args.imbalance, args.seed)
@@ -84,6 +94,7 @@ def main():
                          "levels": st["levels"], "coarsest_n": st["coarsest_n"],
                          "refine_iters": st["refine_iters"], "seconds": round(dt, 1), "cores": 1}
         print("oracle:", rec["oracle"], flush=True)
+        save()
         del part
     if not args.skip_metis:
         mpart, mcut, t_metis = oracle.metis(rp, ci, args.k, seed=args.seed)
@@ -93,9 +104,7 @@ def main():
                         "cores": 1, "library": "METIS 5 (CUDA toolkit libmetis_static.a), METIS_PartGraphKway, "
                                                "64-bit idx_t, default options (ufactor 30), seed 0"}
         print("metis:", rec["metis"], flush=True)
-    with open(args.out, "w") as f:
-        json.dump(rec, f, indent=1)
-        f.write("\n")
+        save()
 
 
 if __name__ == "__main__":

@@ -178,3 +178,70 @@ def test_edge_case_parity(oracle_mod, gp, cuda, name, g, k, imb, w):
     assert s_ref["cut"] == s_gpu["cut"] and s_ref["max_part_weight"] == s_gpu["max_part_weight"]
     cut, pw = gp.edge_cut(d(rp), d(ci), p_gpu, k, ewgt=d(ew), vwgt=d(vw))
     assert cut == s_gpu["cut"] and int(pw.max()) == s_gpu["max_part_weight"]
+
+
+# ---- the co-purchase-shaped configuration at its full size: Chung-Lu graph
+# drawn on 262,111 vertices with ~900k undirected edges (degree exponent 2.5,
+# maximum expected degree 420); the 7,236 vertices left isolated are dropped,
+# as the reference's preprocessing does, leaving 254,875.  k swept over 2..64,
+# unit weights, 3 % imbalance.  k = 64 compares every trace event; the other
+# k compare the final partition and statistics.
+CL_KS = (2, 4, 8, 16, 32, 64)
+
+
+@pytest.fixture(scope="module")
+def chunglu_config():
+    rp, ci = to_np(*graphs.chung_lu())
+    assert len(rp) - 1 == 254875 and len(ci) // 2 == 899727
+    return rp, ci
+
+
+@pytest.mark.parametrize("k", CL_KS)
+def test_chunglu_config_k_sweep(oracle_mod, gp, cuda, chunglu_config, k):
+    rp, ci = chunglu_config
+    trace = k == 64
+    p_ref, s_ref, ev_ref = oracle_mod.partition(rp, ci, k, 0.03, 0, trace=trace)
+    p_gpu, s_gpu, ev_gpu = gp.partition(torch.from_numpy(rp).to(cuda), torch.from_numpy(ci).to(cuda), k, 0.03, 0,
+                                        trace=trace)
+    if trace:
+        compare_traces(ev_ref, ev_gpu)
+    assert np.array_equal(p_ref, p_gpu.cpu().numpy())
+    for key in ("cut", "max_part_weight", "max_allowed", "levels", "coarsest_n", "best_trial", "refine_iters"):
+        assert s_ref[key] == s_gpu[key], (key, s_ref[key], s_gpu[key])
+    assert s_gpu["max_part_weight"] <= s_gpu["max_allowed"]
+
+
+def test_rmat20_k64_matches_oracle(oracle_mod, gp, cuda):
+    """R-MAT scale 20 (646k vertices, 15.7M undirected edges), k = 64: the
+    largest R-MAT the oracle finishes in about half a minute, bit-exact."""
+    rp, ci = graphs.rmat(20, 16, seed=0)[:2]
+    p_ref, s_ref, _ = oracle_mod.partition(rp.numpy(), ci.numpy(), 64, 0.03, 0)
+    p_gpu, s_gpu, _ = gp.partition(rp.to(cuda), ci.to(cuda), 64, 0.03, 0)
+    assert np.array_equal(p_ref, p_gpu.cpu().numpy())
+    for key in ("cut", "max_part_weight", "levels", "coarsest_n", "refine_iters"):
+        assert s_ref[key] == s_gpu[key], (key, s_ref[key], s_gpu[key])
+
+
+def test_headline_config_matches_full_fixture(gp, cuda):
+    """R-MAT scale 24, k = 64 (the benchmark workload, 260M undirected edges):
+    the graph generated on the device and the partition of it are the ones
+    the oracle recorded in tests/golden/rmat24_ef16_k64_full.json (SHA-256 of
+    the CSR and of the part array, cut, heaviest part, levels)."""
+    import hashlib
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rmat24_ef16_k64_full.json")
+    with open(path) as f:
+        fx = json.load(f)
+    rp, ci, _ = graphs.rmat(24, 16, seed=0, device=cuda)
+    def sha(*ts):
+        h = hashlib.sha256()
+        for t in ts:
+            h.update(t.cpu().numpy().view(np.uint8).data)
+        return h.hexdigest()
+    assert sha(rp, ci) == fx["graph"]["sha256_rowptr_colidx"]
+    part, st, _ = gp.partition(rp, ci, 64, 0.03, 0)
+    orc = fx["oracle"]
+    assert (st["cut"], st["max_part_weight"], st["levels"], st["coarsest_n"]) == \
+        (orc["cut"], orc["max_part_weight"], orc["levels"], orc["coarsest_n"])
+    assert sha(part) == orc["sha256_part"]

@@ -300,6 +300,8 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
         B.part = c.keep_alloc<int32_t>(n0);
         B.part_next = c.keep_alloc<int32_t>(n0);
         B.best = c.keep_alloc<int32_t>(n0);
+        B.pc = c.keep_alloc<uint16_t>(n0);
+        B.pc_next = c.keep_alloc<uint16_t>(n0);
         B.dest = c.keep_alloc<int32_t>(n0);
         B.gain = c.keep_alloc<int32_t>(n0);
         B.lock = c.keep_alloc<uint8_t>(n0);

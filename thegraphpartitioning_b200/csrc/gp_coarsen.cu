@@ -552,14 +552,18 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // coalesced.  Tiers by row length d:
 //   A  d <= 128        one warp, 256-slot table in shared memory
 //   B  d <= 1024       one warp, 2048-slot table in shared memory
-//   C  d <= 4096       one CTA, two-phase (first position by atomicMin), table on chip
-//   D  longer          one CTA, two-phase, table in global memory
+//   C  d <= 4096       one CTA of 256 threads, two-phase (first position kept by
+//                      atomicMax of deg - j), 8192-slot table on chip
+//   C2 d <= 12288      the same with 1024 threads and a 16384-slot table (196 KB:
+//                      one CTA per SM; load factor at most 3/4)
+//   D  longer          pieces of 64K entries, one CTA each, table in global memory
 // A and B insert 32 entries at a time in walk order (match_any leaders), so
 // new neighbours get consecutive ranks; C and D rank first positions with one
 // block scan over per-thread contiguous segments.
 constexpr int TA_ROW = 128, TA_SLOTS = 256;
 constexpr int TB_ROW = 1024, TB_SLOTS = 2048, TB_WARPS = 4;
 constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 256;
+constexpr int TC2_ROW = 12288, TC2_SLOTS = 16384, TC2_T = 1024;
 constexpr int TD_T = 1024;
 constexpr int32_t EMPTY_KEY = -1;
 
@@ -709,16 +713,20 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
     return r;
 }
 
-// rows longer than TB_ROW: list (TC_ROW-bounded rows first use the on-chip table)
-// count[0] = rows of tier C, count[1] = rows of tier D, count[2] = longest tier-D row
+// rows longer than TB_ROW: lists of the on-chip tiers C (<= TC_ROW) and C2
+// (<= TC2_ROW) and of tier D.  count[0] = rows of tier C, count[1] = rows of
+// tier D, count[2] = longest tier-D row, count[3] = rows of tier C2
 __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC,
-                            int32_t* __restrict__ listD, int64_t* __restrict__ count) {
+                            int32_t* __restrict__ listC2, int32_t* __restrict__ listD, int64_t* __restrict__ count) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = cdeg[c];
         if (d <= TB_ROW) continue;
         if (d <= TC_ROW) {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[0], 1ull);
             listC[slot] = (int32_t)c;
+        } else if (d <= TC2_ROW) {
+            unsigned long long slot = atomicAdd((unsigned long long*)&count[3], 1ull);
+            listC2[slot] = (int32_t)c;
         } else {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[1], 1ull);
             listD[slot] = (int32_t)c;
@@ -820,23 +828,32 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(TC_T) k_dedup_cta_smem(const int32_t* __restrict__ list, int64_t nlist,
-                                                         const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                         const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
-                                                         int32_t* __restrict__ tci, int32_t* __restrict__ tew,
-                                                         int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+// shared memory of an on-chip tier: SLOTS 64-bit slots and int32 weight sums,
+// two words per 32 entries of the longest row
+template <int SLOTS, int MAXROW>
+constexpr size_t cta_dedup_smem() {
+    return (sizeof(unsigned long long) + sizeof(int32_t)) * SLOTS + sizeof(int32_t) * 2 * ((MAXROW + 31) / 32);
+}
+
+// tiers C and C2: table of at least twice the row length, at most SLOTS
+template <int T, int SLOTS, int MAXROW>
+__global__ void __launch_bounds__(T) k_dedup_cta_smem(const int32_t* __restrict__ list, int64_t nlist,
+                                                      const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
+                                                      const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
+                                                      int32_t* __restrict__ tci, int32_t* __restrict__ tew,
+                                                      int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char stab_raw[];
-    unsigned long long* slot = (unsigned long long*)stab_raw;          // TC_SLOTS
-    int32_t* wsum = (int32_t*)(slot + TC_SLOTS);                       // TC_SLOTS
-    int32_t* words = wsum + TC_SLOTS;                                  // 2 * TC_ROW / 32
+    unsigned long long* slot = (unsigned long long*)stab_raw;          // SLOTS
+    int32_t* wsum = (int32_t*)(slot + SLOTS);                          // SLOTS
+    int32_t* words = wsum + SLOTS;                                     // 2 * MAXROW / 32
     __shared__ int32_t sh[33];
     for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int64_t c = list[li];
         const int64_t deg = cdeg[c];
         int64_t S = 1;
         int lg = 0;
-        while (S < 2 * deg) { S <<= 1; ++lg; }
-        cta_dedup<TC_T>(mapped, mw, off[c], deg, (int32_t)c, slot, wsum, S, lg, words, tci, tew, &cnt[c], sh, err);
+        while (S < 2 * deg && S < SLOTS) { S <<= 1; ++lg; }
+        cta_dedup<T>(mapped, mw, off[c], deg, (int32_t)c, slot, wsum, S, lg, words, tci, tew, &cnt[c], sh, err);
     }
 }
 
@@ -1014,10 +1031,11 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int32_t* tew = c.tmp_alloc<int32_t>(T);
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
     int32_t* listC = c.tmp_alloc<int32_t>(nc);
+    int32_t* listC2 = c.tmp_alloc<int32_t>(nc);
     int32_t* listD = c.tmp_alloc<int32_t>(nc);
-    int64_t* lcount = c.tmp_alloc<int64_t>(3);
+    int64_t* lcount = c.tmp_alloc<int64_t>(4);
     int32_t* err = c.tmp_alloc<int32_t>(1);
-    memset_async(c, lcount, 0, 3 * sizeof(int64_t));
+    memset_async(c, lcount, 0, 4 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
         const int grid = (int)fine.nitems + grid_for(g.n * 32, 256, c.sm_count * c.ctas_per_sm);
@@ -1036,16 +1054,22 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
                                                                                         mapped, mw, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
-    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listD, lcount);
+    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listD, lcount);
     GP_LAUNCHED(c);
-    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
     c.sync();
-    const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2];
+    const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2], nC2 = c.h_pinned[3];
     if (nC > 0) {
-        const size_t smem = (sizeof(unsigned long long) + sizeof(int32_t)) * TC_SLOTS + sizeof(int32_t) * 2 * ((TC_ROW + 31) / 32);
         // one CTA per row: the block scheduler balances rows of unequal length
-        k_dedup_cta_smem<<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * c.ctas_per_sm), TC_T, smem, c.s>>>(
-            listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
+        k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>
+            <<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * c.ctas_per_sm), TC_T,
+               cta_dedup_smem<TC_SLOTS, TC_ROW>(), c.s>>>(listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
+        GP_LAUNCHED(c);
+    }
+    if (nC2 > 0) {
+        k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>
+            <<<(unsigned)std::min<int64_t>(nC2, (int64_t)c.sm_count * c.ctas_per_sm), TC2_T,
+               cta_dedup_smem<TC2_SLOTS, TC2_ROW>(), c.s>>>(listC2, nC2, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
     if (nD > 0) {
@@ -1137,12 +1161,14 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
 void coarsen_smem_caps() {
     constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
     constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
-    const size_t smC = (sizeof(unsigned long long) + sizeof(int32_t)) * TC_SLOTS + sizeof(int32_t) * 2 * ((TC_ROW + 31) / 32);
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smA));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
-    GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smC));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_dedup_smem<TC_SLOTS, TC_ROW>()));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_dedup_smem<TC2_SLOTS, TC2_ROW>()));
 }
 
 }  // namespace gp

@@ -92,6 +92,9 @@ struct RefineBufs {
     int32_t* part = nullptr;
     int32_t* part_next = nullptr;
     int32_t* best = nullptr;
+    void* pc = nullptr;           // uint8 / uint16 copy of part read by the neighbour gathers
+    void* pc_next = nullptr;      // and of part_next
+    int pcb = 1;                  // its bytes per vertex (1: k <= 256, 2: k <= 1024)
     int32_t* dest = nullptr;
     int32_t* gain = nullptr;
     uint8_t* lock = nullptr;

@@ -96,12 +96,28 @@ struct ConnArgs {
     int32_t* gain;
     int32_t* part_next;         // label propagation: part and cleared lock copied here for the
     uint8_t* lock_next;         // move step (nullptr: not needed)
+    const void* pc;             // the part array as gathered per neighbour: PT[n], a uint8 or uint16
+                                // copy of part (k <= 256 / k <= 1024), or part itself (int32)
+    void* pc_next;              // copy of part_next in the same type (nullptr: none kept)
     int64_t* status;
     int32_t* clist[3];
     int32_t* hhist;
     int64_t* hsum;
     int32_t* hdone;
 };
+
+// part id of neighbour u from the gather copy (read-only in the kernel)
+template <class PT>
+__device__ __forceinline__ int32_t gpart(const void* pc, int32_t u) {
+    return (int32_t)__ldg((const PT*)pc + u);
+}
+
+// rebalance moves keep the gather copy of part current (pcb bytes per id)
+__device__ __forceinline__ void store_pc(void* pc, int pcb, int64_t v, int32_t d) {
+    if (!pc) return;
+    if (pcb == 1) ((uint8_t*)pc)[v] = (uint8_t)d;
+    else ((uint16_t*)pc)[v] = (uint16_t)d;
+}
 
 __device__ __forceinline__ void hist_add(int32_t* hist, int32_t q, int32_t w, bool valid) {
     if (valid) atomicAdd(&hist[q], w);
@@ -120,9 +136,13 @@ __device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, i
 
 // decision of one row from its best other part (bq, bk), own connectivity
 // and total weighted degree; returns true when an LP candidate is recorded
+template <class PT>
 __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool active, int64_t v, int32_t p,
                                             int64_t tot, int64_t cross, uint64_t bk, int32_t bq, int32_t light) {
-    if (mode == MODE_LP && A.part_next) { A.part_next[v] = p; A.lock_next[v] = 0; }
+    if (mode == MODE_LP && A.part_next) {
+        A.part_next[v] = p; A.lock_next[v] = 0;
+        if (A.pc_next) ((PT*)A.pc_next)[v] = (PT)p;
+    }
     const int64_t own = tot - cross;
     int32_t d = -1, gn = 0;
     bool cand = false;
@@ -142,7 +162,7 @@ __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool ac
 }
 
 // rows of at most TILE entries, TILE lanes per row, 32/TILE rows per warp
-template <int TILE>
+template <int TILE, class PT>
 __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
                                           int list_id, int64_t& acc) {
     const int lane = threadIdx.x & 31, tl = lane & (TILE - 1), tix = lane / TILE;
@@ -157,7 +177,7 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     const int64_t e = beg + tl;
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
-    if (has) { q = A.part[__ldcs(&A.g.ci[e])]; w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
+    if (has) { q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e])); w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
     const uint32_t tmask = TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (tix * TILE));
     const int32_t cross = (int32_t)__reduce_add_sync(tmask, (has && q != p) ? (uint32_t)w : 0u);
     const int32_t tot = (int32_t)__reduce_add_sync(tmask, (uint32_t)w);
@@ -171,7 +191,7 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     bool take = false;
     if (tl == 0 && v >= 0) {
         acc += cross;
-        take = conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light);
+        take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
         if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
     warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))]);
@@ -185,6 +205,7 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
 // otherwise over the row's entries again (same candidates: parts with a
 // non-zero connection).
 constexpr int kBinsK = 256;
+template <class PT>
 __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
                                           int32_t* hist, int64_t& acc) {
     const int lane = threadIdx.x & 31;
@@ -201,7 +222,7 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
             w[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
         }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? A.part[u[c]] : -1;
+        for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? gpart<PT>(A.pc, u[c]) : -1;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             tot += w[c];
@@ -227,24 +248,25 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
             for (int q = lane; q < A.k; q += 32) hist[q] = 0;
         } else {
             for (int64_t e = beg + lane; e < end; e += 32) {
-                const int32_t q = A.part[__ldcs(&A.g.ci[e])];
+                const int32_t q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]));
                 if (q != p && (mode != MODE_RB || !over[q])) argmax_u32(lh, lq, (uint32_t)hist[q], q);
             }
             group_argmax_u32(0xffffffffu, bk, bq, lh, lq);
             __syncwarp();
-            for (int64_t e = beg + lane; e < end; e += 32) hist[A.part[__ldcs(&A.g.ci[e])]] = 0;
+            for (int64_t e = beg + lane; e < end; e += 32) hist[gpart<PT>(A.pc, __ldcs(&A.g.ci[e]))] = 0;
         }
         __syncwarp();
     }
     bool take = false;
     if (lane == 0) {
         acc += cross;
-        take = conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light);
+        take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
         if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
     warp_push(take, (int32_t)v, A.clist[2], &A.status[S_NL2]);
 }
 
+template <class PT>
 __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
     extern __shared__ int32_t csm[];
     const int32_t k = A.k;
@@ -308,7 +330,7 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
                 ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
             }
 #pragma unroll
-            for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
+            for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? gpart<PT>(A.pc, uu[c]) : -1;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 tot += ww[c];
@@ -368,7 +390,7 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
             if (threadIdx.x == 0) {
                 for (int i = 1; i < RW; ++i) argmax_q(bk, bq, s_k[i], s_q[i]);
                 const int64_t rdeg = A.g.rp[v + 1] - A.g.rp[v];
-                if (conn_decide(A, mode, active, v, p, tot, cross, bk, bq, light))
+                if (conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light))
                     atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)rdeg);
             }
         }
@@ -390,12 +412,12 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
         const int64_t u0 = first_unit((T * wid) / nw), u1 = first_unit((T * (wid + 1)) / nw);
         for (int64_t u = u0; u < u1; ++u) {
             if (u < U2) {
-                conn_warp(A, A.bucket[2][u], mode, over, light, hist, acc);
+                conn_warp<PT>(A, A.bucket[2][u], mode, over, light, hist, acc);
             } else if (u < U2 + U1) {
-                conn_tile<kTile32>(A, A.bucket[1][u - U2], mode, over, light, 1, acc);
+                conn_tile<kTile32, PT>(A, A.bucket[1][u - U2], mode, over, light, 1, acc);
             } else {
                 const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
+                conn_tile<kTile8, PT>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
             }
         }
     }
@@ -411,11 +433,12 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
 }
 
 // ------------------------------------------------------------------ LP apply
+template <class PT>
 __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v, int32_t p, int32_t d, int32_t gv,
-                                           const int32_t* __restrict__ part, const int32_t* __restrict__ dest,
+                                           const void* pc, const int32_t* __restrict__ dest,
                                            const int32_t* __restrict__ gain) {
     const int32_t u = __ldcs(&g.ci[e]);
-    int32_t pu = part[u];
+    int32_t pu = gpart<PT>(pc, u);
     const int32_t du = dest[u];
     if (du >= 0) {
         const int32_t gu = gain[u];
@@ -441,15 +464,19 @@ struct ApplyArgs {
     const int64_t* status;
     int32_t* part_next;
     uint8_t* lock_next;
+    const void* pc;             // gather copy of part (as in ConnArgs)
+    void* pc_next;              // its copy of part_next (nullptr: none kept)
     int64_t* pw;
     int64_t* moves_out;
     int64_t* hsum;
     int32_t* hdone;
 };
 
+template <class PT>
 __device__ __forceinline__ void ab_commit(const ApplyArgs& A, int64_t v, int32_t p, int32_t d, int64_t* delta,
                                           int64_t& moves) {
     A.part_next[v] = d;
+    if (A.pc_next) ((PT*)A.pc_next)[v] = (PT)d;
     A.lock_next[v] = 1;
     const int64_t wv = A.g.vw ? A.g.vw[v] : 1;
     atomicAdd((unsigned long long*)&delta[d], (unsigned long long)wv);
@@ -458,7 +485,7 @@ __device__ __forceinline__ void ab_commit(const ApplyArgs& A, int64_t v, int32_t
 }
 
 // candidate rows of at most TILE entries, TILE lanes each
-template <int TILE>
+template <int TILE, class PT>
 __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
     const int lane = threadIdx.x & 31, tl = lane & (TILE - 1);
     int32_t t = 0, p = -1, d = -1;
@@ -466,14 +493,15 @@ __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* 
         d = A.dest[v]; p = A.part[v];
         const int32_t gv = A.gain[v];
         const int64_t e = A.g.rp[v] + tl;
-        if (e < A.g.rp[v + 1]) t = ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
+        if (e < A.g.rp[v + 1]) t = ab_term<PT>(A.g, e, v, p, d, gv, A.pc, A.dest, A.gain);
     }
 #pragma unroll
     for (int o = TILE / 2; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (tl == 0 && v >= 0 && t >= 0) ab_commit(A, v, p, d, delta, moves);
+    if (tl == 0 && v >= 0 && t >= 0) ab_commit<PT>(A, v, p, d, delta, moves);
 }
 
 // one candidate row of 33..kHeavyDeg entries per warp, 128 entries per sweep
+template <class PT>
 __device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
     const int lane = threadIdx.x & 31;
     const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
@@ -489,7 +517,7 @@ __device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* 
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            pu[c] = uu[c] >= 0 ? A.part[uu[c]] : -1;
+            pu[c] = uu[c] >= 0 ? gpart<PT>(A.pc, uu[c]) : -1;
             du[c] = uu[c] >= 0 ? A.dest[uu[c]] : -1;
         }
 #pragma unroll
@@ -504,9 +532,10 @@ __device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* 
         }
     }
     g2 = warp_sum(g2);
-    if (lane == 0 && g2 >= 0) ab_commit(A, v, p, d, delta, moves);
+    if (lane == 0 && g2 >= 0) ab_commit<PT>(A, v, p, d, delta, moves);
 }
 
+template <class PT>
 __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
     extern __shared__ int64_t delta[];
     __shared__ int64_t s_red[RW];
@@ -523,7 +552,7 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
             const int32_t p = A.part[v], gv = A.gain[v];
             int32_t g2 = 0;
             for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < A.item_end[blockIdx.x]; e += RT)
-                g2 += ab_term(A.g, e, v, p, d, gv, A.part, A.dest, A.gain);
+                g2 += ab_term<PT>(A.g, e, v, p, d, gv, A.pc, A.dest, A.gain);
             g2 = warp_sum(g2);
             if (lane == 0) s_red[w] = g2;
             __syncthreads();
@@ -542,7 +571,7 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
                         A.hdone[h] = 0;
                     }
                 }
-                if (last && sum >= 0) ab_commit(A, v, p, d, delta, moves);
+                if (last && sum >= 0) ab_commit<PT>(A, v, p, d, delta, moves);
             }
         }
     } else {
@@ -553,11 +582,11 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
         for (int64_t u = wid; u < U0 + n1 + n2; u += nw) {
             if (u < U0) {
                 const int64_t i = u * 4 + (lane >> 3);
-                ab_tile<kTile8>(A, i < n0 ? A.clist[0][i] : -1, delta, moves);
+                ab_tile<kTile8, PT>(A, i < n0 ? A.clist[0][i] : -1, delta, moves);
             } else if (u < U0 + n1) {
-                ab_tile<kTile32>(A, A.clist[1][u - U0], delta, moves);
+                ab_tile<kTile32, PT>(A, A.clist[1][u - U0], delta, moves);
             } else {
-                ab_warp(A, A.clist[2][u - U0 - n1], delta, moves);
+                ab_warp<PT>(A, A.clist[2][u - U0 - n1], delta, moves);
             }
         }
     }
@@ -630,7 +659,8 @@ __global__ void k_rb_rekey(int64_t cnt, const uint64_t* __restrict__ keys, const
 __global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals,
                                 const int64_t* __restrict__ pre, const int32_t* __restrict__ vw,
                                 const int64_t* __restrict__ pw_snap, int64_t Lmax, int32_t* __restrict__ part,
-                                uint8_t* __restrict__ lock, int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
+                                void* pc, int pcb, uint8_t* __restrict__ lock, int64_t* __restrict__ pw,
+                                int64_t* __restrict__ moves) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t d = keys[i] >> RB_SHIFT;
         const int64_t s = seg_start(keys, i, d);
@@ -639,6 +669,7 @@ __global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, 
         if ((pre[i] - pre[s]) + wv <= Lmax - pw_snap[d]) {
             const int32_t p = part[v];
             part[v] = (int32_t)d; lock[v] = 1;
+            store_pc(pc, pcb, v, (int32_t)d);
             atomicAdd((unsigned long long*)&pw[d], (unsigned long long)wv);
             atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
             atomicAdd((unsigned long long*)moves, 1ull);
@@ -667,7 +698,8 @@ __global__ void k_mask_vw(int64_t cnt, const int32_t* __restrict__ flag, const i
 __global__ void k_rb_strong_apply(int64_t cnt, const int32_t* __restrict__ vals, const int32_t* __restrict__ flag,
                                   const int64_t* __restrict__ P, const int32_t* __restrict__ vw,
                                   const int64_t* __restrict__ cum, int32_t k, int32_t* __restrict__ part,
-                                  uint8_t* __restrict__ lock, int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
+                                  void* pc, int pcb, uint8_t* __restrict__ lock, int64_t* __restrict__ pw,
+                                  int64_t* __restrict__ moves) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
         const int64_t pre = P[i];
@@ -684,6 +716,7 @@ __global__ void k_rb_strong_apply(int64_t cnt, const int32_t* __restrict__ vals,
         if (q < k && pre + wv <= cum[q + 1]) {
             const int32_t p = part[v];
             part[v] = q; lock[v] = 1;
+            store_pc(pc, pcb, v, q);
             atomicAdd((unsigned long long*)&pw[q], (unsigned long long)wv);
             atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
             atomicAdd((unsigned long long*)moves, 1ull);
@@ -876,6 +909,8 @@ __device__ __forceinline__ int cta_seg_start(const uint64_t* a, int i, int shift
 struct RbCta {
     const int32_t* vw;
     int32_t* part;
+    void* pc;                   // gather copy of part to keep current (nullptr: none)
+    int pcb;                    // its bytes per id
     uint8_t* lock;
     const int32_t* dest;
     const int32_t* gain;
@@ -947,6 +982,7 @@ __device__ int64_t cta_rebalance(const RbCta& R, int mode, int64_t n, const int3
             if ((R.pre[i] - R.pre[s0]) + wv <= Lmax - s_snap[d]) {
                 const int32_t p = part[v];
                 part[v] = d; lock[v] = 1;
+                store_pc(R.pc, R.pcb, v, d);
                 atomicAdd((unsigned long long*)&s_pw[d], (unsigned long long)wv);
                 atomicAdd((unsigned long long*)&s_pw[p], (unsigned long long)(-wv));
                 ++moves;
@@ -977,6 +1013,7 @@ __device__ int64_t cta_rebalance(const RbCta& R, int mode, int64_t n, const int3
             if (lo < k && pre + wv <= s_cum[lo + 1]) {
                 const int32_t p = part[v];
                 part[v] = lo; lock[v] = 1;
+                store_pc(R.pc, R.pcb, v, lo);
                 atomicAdd((unsigned long long*)&s_pw[lo], (unsigned long long)wv);
                 atomicAdd((unsigned long long*)&s_pw[p], (unsigned long long)(-wv));
                 ++moves;
@@ -1065,15 +1102,16 @@ __global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
         CA.unit_cost = nullptr; CA.nunits = 0;
         CA.dest = R.dest; CA.gain = R.gain; CA.status = R.status;
         CA.part_next = nullptr; CA.lock_next = nullptr;
+        CA.pc = part; CA.pc_next = nullptr;
         CA.hhist = nullptr; CA.hsum = nullptr; CA.hdone = nullptr;
         int64_t acc = 0;
         int32_t* hist = s_hist + w * k;
         for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
-            if (u < U2) conn_warp(CA, R.bucket[2][u], dmode, s_over, light, hist, acc);
-            else if (u < U2 + U1) conn_tile<kTile32>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, acc);
+            if (u < U2) conn_warp<int32_t>(CA, R.bucket[2][u], dmode, s_over, light, hist, acc);
+            else if (u < U2 + U1) conn_tile<kTile32, int32_t>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, acc);
             else {
                 const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, acc);
+                conn_tile<kTile8, int32_t>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, acc);
             }
         }
         acc = warp_sum(acc);
@@ -1119,18 +1157,19 @@ __global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
             AA.item_row = nullptr; AA.item_beg = nullptr; AA.item_end = nullptr; AA.row_items = nullptr; AA.nitems = 0;
             for (int b = 0; b < 3; ++b) AA.clist[b] = R.clist[b];
             AA.status = R.status; AA.part_next = part_next; AA.lock_next = lock_next; AA.pw = nullptr;
+            AA.pc = part; AA.pc_next = nullptr;
             AA.moves_out = nullptr; AA.hsum = nullptr; AA.hdone = nullptr;
             for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
                 if (u < U2) {
                     const int64_t v = R.bucket[2][u];
-                    if (R.dest[v] >= 0) ab_warp(AA, v, s_pw, moves);
+                    if (R.dest[v] >= 0) ab_warp<int32_t>(AA, v, s_pw, moves);
                 } else if (u < U2 + U1) {
                     const int64_t v = R.bucket[1][u - U2];
-                    ab_tile<kTile32>(AA, R.dest[v] >= 0 ? v : -1, s_pw, moves);
+                    ab_tile<kTile32, int32_t>(AA, R.dest[v] >= 0 ? v : -1, s_pw, moves);
                 } else {
                     const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
                     const int64_t v = i < R.nbucket[0] ? R.bucket[0][i] : -1;
-                    ab_tile<kTile8>(AA, (v >= 0 && R.dest[v] >= 0) ? v : -1, s_pw, moves);
+                    ab_tile<kTile8, int32_t>(AA, (v >= 0 && R.dest[v] >= 0) ? v : -1, s_pw, moves);
                 }
             }
             nmoves = cta_sum(moves, sh);
@@ -1140,7 +1179,8 @@ __global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
             for (int64_t v = threadIdx.x; v < n; v += CT) lock[v] = 0;
             __syncthreads();
             RbCta RA;
-            RA.vw = R.g.vw; RA.part = part; RA.lock = lock; RA.dest = R.dest; RA.gain = R.gain; RA.pre = R.pre;
+            RA.vw = R.g.vw; RA.part = part; RA.pc = nullptr; RA.pcb = 0; RA.lock = lock; RA.dest = R.dest;
+            RA.gain = R.gain; RA.pre = R.pre;
             RA.flag = R.flag; RA.gkeys = R.gkeys; RA.k = k; RA.Lmax = Lmax;
             moves = cta_rebalance(RA, mode, n, nullptr, 0, s_pw, s_snap, s_cum, s_keys, sh);
             nmoves = cta_sum(moves, sh);
@@ -1248,6 +1288,12 @@ static void trace_iter(Ctx& c, const RefineBufs& B, int64_t n, int64_t m, int le
     tr.emit(ev);
 }
 
+// the part array as the neighbour gathers read it: 1 or 2 bytes per vertex
+__global__ void k_compact_part(int64_t n, const int32_t* __restrict__ part, void* pc, int pcb) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        store_pc(pc, pcb, v, part[v]);
+}
+
 int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr) {
     if (cta_refine_ok(L, P)) return refine_level_cta(c, L, P, B, level, tr);
     const DGraph& g = L.g;
@@ -1255,6 +1301,13 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const int32_t k = P.k;
     const int64_t Lmax = P.Lmax;
     memset_async(c, B.lock, 0, n);
+    // neighbour gathers read a uint8 (k <= 256) or uint16 copy of part, kept
+    // current by every step that moves vertices: a quarter or half of the
+    // bytes per gather, and of the array that has to stay in L2
+    B.pcb = k <= 256 ? 1 : 2;
+    k_compact_part<<<grid_for(n, 256), 256, 0, c.s>>>(n, B.part, B.pc, B.pcb);
+    GP_LAUNCHED(c);
+    c.bytes += 4 * n + B.pcb * n;
     const int kpad = (k + 15) & ~15;
     const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
     // at most 1024 + 32 * GP_MAX_K bytes: below the 48 KB default, no attribute needed
@@ -1277,11 +1330,13 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         CA.unit_cost = L.unit_cost; CA.nunits = L.nunits;
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
         CA.part_next = B.part_next; CA.lock_next = B.lock_next;   // the LP step's starting copy
-        k_conn<<<grid, RT, conn_smem, c.s>>>(CA);
+        CA.pc = B.pc; CA.pc_next = B.pc_next;
+        if (B.pcb == 1) k_conn<uint8_t><<<grid, RT, conn_smem, c.s>>>(CA);
+        else k_conn<uint16_t><<<grid, RT, conn_smem, c.s>>>(CA);
         GP_LAUNCHED(c);
         if (c.profile) GP_CUDA(cudaEventRecord(c.ev_b, c.s));
-        // rowptr, colidx, weights, gathered part[u]; part[v], lock[v] read; dest, gain written
-        const int64_t conn_bytes = L.scan_bytes() + 4 * n + n + 8 * n;
+        // rowptr, colidx, weights, gathered part[u] (pcb bytes); part[v], lock[v] read; dest, gain written
+        const int64_t conn_bytes = L.scan_bytes() - (4 - B.pcb) * g.m + 4 * n + n + 8 * n;
         c.bytes += conn_bytes;
         GP_CUDA(cudaMemcpyAsync(c.h_pinned, B.status, sizeof(int64_t) * S_NSLOTS, cudaMemcpyDeviceToHost, c.s));
         c.sync();
@@ -1339,17 +1394,21 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             for (int b = 0; b < 3; ++b) AA.clist[b] = B.clist[b];
             AA.status = B.status; AA.part_next = B.part_next; AA.lock_next = B.lock_next; AA.pw = B.pw;
             AA.moves_out = moves_d;
-            k_lp_apply<<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
+            AA.pc = B.pc; AA.pc_next = B.pc_next;
+            if (B.pcb == 1) k_lp_apply<uint8_t><<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
+            else k_lp_apply<uint16_t><<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
             GP_LAUNCHED(c);
-            // copy pass + afterburner: candidate rows with three gathered int32 per entry
-            c.bytes += 9 * n + 16 * nlist + cdeg * (4 + (g.ew ? 4 : 0) + 12);
+            // copy pass + afterburner: candidate rows with gathered part (pcb bytes), dest and gain per entry
+            c.bytes += (9 + B.pcb) * n + 16 * nlist + cdeg * (4 + (g.ew ? 4 : 0) + 8 + B.pcb);
             std::swap(B.part, B.part_next);
             std::swap(B.lock, B.lock_next);
+            std::swap(B.pc, B.pc_next);
         } else if (n <= kCtaMaxN) {
             // the whole step in one thread block
             auto mk = c.tmp->save();
             RbCta RA;
-            RA.vw = g.vw; RA.part = B.part; RA.lock = B.lock; RA.dest = B.dest; RA.gain = B.gain;
+            RA.vw = g.vw; RA.part = B.part; RA.pc = B.pc; RA.pcb = B.pcb; RA.lock = B.lock; RA.dest = B.dest;
+            RA.gain = B.gain;
             RA.pre = c.tmp_alloc<int64_t>(n); RA.flag = c.tmp_alloc<int32_t>(n); RA.gkeys = c.tmp_alloc<uint64_t>(n);
             RA.k = k; RA.Lmax = Lmax;
             k_rb_step_cta<<<1, CT, cta_refine_smem(k), c.s>>>(RA, mode, n, nullptr, 0, B.pw, moves_d);
@@ -1372,7 +1431,8 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                 k_rb_compact<<<grid_for(n, 256), 256, 0, c.s>>>(n, flag, vpos, B.part, B.gain, B.ckeys, B.cvals);
                 GP_LAUNCHED(c);
                 RbCta RA;
-                RA.vw = g.vw; RA.part = B.part; RA.lock = B.lock; RA.dest = B.dest; RA.gain = B.gain;
+                RA.vw = g.vw; RA.part = B.part; RA.pc = B.pc; RA.pcb = B.pcb; RA.lock = B.lock; RA.dest = B.dest;
+                RA.gain = B.gain;
                 RA.pre = c.tmp_alloc<int64_t>(ncand); RA.flag = c.tmp_alloc<int32_t>(ncand);
                 RA.gkeys = c.tmp_alloc<uint64_t>(ncand); RA.k = k; RA.Lmax = Lmax;
                 k_rb_step_cta<<<1, CT, cta_refine_smem(k), c.s>>>(RA, mode, n, B.cvals, ncand, B.pw, moves_d);
@@ -1406,7 +1466,8 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                         GP_LAUNCHED(c);
                         scan_excl_i32_to_i64(c, wv, pre, n2, nullptr);
                         k_rb_weak_apply<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.ckeys2, B.cvals2, pre, g.vw, pw_snap,
-                                                                           Lmax, B.part, B.lock, B.pw, moves_d);
+                                                                           Lmax, B.part, B.pc, B.pcb, B.lock, B.pw,
+                                                                           moves_d);
                         GP_LAUNCHED(c);
                     }
                 } else {
@@ -1418,7 +1479,8 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                     GP_LAUNCHED(c);
                     scan_excl_i32_to_i64(c, wm, pre, ncand, nullptr);
                     k_rb_strong_apply<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, acc, pre, g.vw, cum, k,
-                                                                           B.part, B.lock, B.pw, moves_d);
+                                                                           B.part, B.pc, B.pcb, B.lock, B.pw,
+                                                                           moves_d);
                     GP_LAUNCHED(c);
                 }
                 c.bytes += 80 * ncand;
