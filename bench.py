@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--sample-scale", type=int, default=17, help="R-MAT scale of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch-sample", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--metis-full", action="store_true", help="also run METIS on the full workload (minutes)")
     ap.add_argument("--workload", default="rmat", choices=["rmat", "batch"],
@@ -262,6 +263,35 @@ def cpu_sample(args):
                            "metis_seconds": t_metis, "metis_cores": 1,
                            "cut_vs_metis": round(gst["cut"] / max(mcut, 1), 4)},
     }
+
+
+def batch_sample(args, dev, count=256):
+    """The batched configuration on a sample: every 16th graph of the 4096-graph
+    batch (the same size mix), timed with CUDA events after one warm call."""
+    import torch
+    import thegraphpartitioning_b200 as gp
+    from thegraphpartitioning_b200 import graphs
+    specs = graphs.batch_specs(4096, seed=args.seed)[::4096 // count][:count]
+    gs = [graphs.batch_graph(sp, device=dev) for sp in specs]
+    ks = [sp["k"] for sp in specs]
+    seeds = [sp["seed"] for sp in specs]
+    outs = [torch.empty(g[0].numel() - 1, dtype=torch.int32, device=dev) for g in gs]
+    gp.partition_batch(gs, ks, args.imbalance, seeds, workers=args.workers, outs=outs)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _, st = gp.partition_batch(gs, ks, args.imbalance, seeds, workers=args.workers, outs=outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    m = sum(g[1].numel() // 2 for g in gs)
+    return {"graphs": len(gs), "sample": "every 16th graph of the 4096-graph batch (RGG + Erdos-Renyi, "
+                                          "n log-uniform in [1k, 200k], k in {2..32})",
+            "vertices": sum(g[0].numel() - 1 for g in gs), "m_undirected": m, "ms": ms,
+            "value": m / (ms / 1e3), "unit": "edges/s", "workers": args.workers,
+            "gpu_launches": int(sum(x["kernel_launches"] for x in st)),
+            "sum_of_cuts": int(sum(x["cut"] for x in st))}
 
 
 def _reference_worker(job):
@@ -582,6 +612,8 @@ def main():
             line.update(full)
         if world == 1 and not args.no_cpu_baseline:
             line.update(cpu_sample(args))
+        if world == 1 and not args.no_batch_sample:
+            line["batch_sample"] = batch_sample(args, dev)
         if args.metis_full:
             import oracle
             mpart, mcut, t_metis = oracle.metis(rp.cpu().numpy(), ci.cpu().numpy(), args.k, seed=args.seed)

@@ -79,7 +79,14 @@ typedef struct gp_options {
                                    large ones; 8 in gp_partition_batch_device, where
                                    concurrent V-cycles share the GPU); results are
                                    identical for every value (autotuner knob)          */
-    int32_t reserved[2];
+    int32_t heavy_deg;          /* rows longer than this many entries are scanned by whole
+                                   CTAs (8 warps), shorter ones by one warp or a lane
+                                   group (0: 2048; 64..65536); results are identical
+                                   for every value (autotuner knob; the learned V-cycle
+                                   always uses the defaults of this and item_len)       */
+    int32_t item_len;           /* entries of one CTA's piece of a long row (0: 16384;
+                                   heavy_deg..1048576); results are identical (autotuner
+                                   knob)                                                */
 } gp_options;
 
 /* Result record of one call. */
@@ -116,7 +123,9 @@ enum gp_trace_kind {
     GP_TR_REFINE_ITER = 4, /* a0 = dest[n] (-1: no proposal), a1 = gain[n],
                               a2 = part[n] after the iteration; cut/maxpw before it   */
     GP_TR_LEVEL_DONE = 5,  /* a0 = part[n] after refinement of this level             */
-    GP_TR_PRIO = 6         /* learned mode: a0 = matching priority per entry (m)       */
+    GP_TR_PRIO = 6,        /* learned mode: a0 = matching priority per entry (m)       */
+    GP_TR_MOVE_PRIO = 7    /* learned mode with a move-order head: a0 = move priority
+                              per vertex (n) of a label-propagation step, before it   */
 };
 
 typedef struct gp_trace_event {
@@ -251,6 +260,30 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
                                 gp_stats* stats, const gp_gnn* model, int32_t fallback, gp_learned_report* report,
                                 gp_trace_fn trace, void* trace_user);
 
+/* Move-order head of the learned mode (no counterpart in the reference): a
+ * second small network (4 features -> 16 hidden -> 1, BF16 weights, FP32
+ * accumulation) scores each label-propagation candidate from its integer
+ * gain, degree, vertex weight and level; the learned V-cycle's afterburner
+ * then assumes the neighbours of higher (score, lower id) move first, in place
+ * of the (gain, id) order.  Only the order changes: every move is still
+ * re-evaluated exactly and the fallback keeps the plain partition unless the
+ * learned one is at least as good.  nparams = 0 removes the head. */
+int gp_gnn_move_num_params(void);
+int gp_gnn_set_move_params(gp_gnn* model, const float* params, int32_t nparams);
+int gp_gnn_get_move_params(const gp_gnn* model, float* params, int32_t nparams);
+/* features of every candidate (d_dest[v] >= 0) of one step: 4 floats per vertex */
+int gp_gnn_move_features_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_vwgt, const int32_t* d_dest,
+                                const int32_t* d_gain, int32_t level, void* stream, float* d_feat_out);
+/* scores (float, may be NULL) and move priorities (int32, may be NULL) of ns feature rows */
+int gp_gnn_move_scores_device(gp_gnn* model, int64_t ns, const float* d_feat, void* stream, float* d_score_out,
+                              int32_t* d_prio_out);
+/* mean binary cross-entropy of ns scored rows against d_label and its gradient (host) */
+int gp_gnn_move_grad_device(gp_gnn* model, int64_t ns, const float* d_feat, const uint8_t* d_label, void* stream,
+                            float* loss_out, float* grad_out);
+/* one Adam step of the head on ns labelled rows */
+int gp_gnn_move_train_step_device(gp_gnn* model, int64_t ns, const float* d_feat, const uint8_t* d_label, float lr,
+                                  void* stream, float* loss_out);
+
 /* Largest k accepted by gp_edge_cut_device_noalloc. */
 #define GP_NOALLOC_MAX_K 1024
 
@@ -272,6 +305,16 @@ int gp_edge_cut_device_noalloc(int64_t n, const int64_t* d_rowptr, const int32_t
                                const int32_t* d_ewgt, const int32_t* d_vwgt,
                                const int32_t* d_part, int32_t k, void* stream,
                                int64_t* cut_out, int64_t* part_weights_out);
+
+/* Bounds-checked build (libgp_b200_checked.so, the same sources compiled with
+ * -DGP_CHECKED; no counterpart in the reference).  Its kernels test
+ * data-dependent indices (neighbour ids, part ids, hash slots, output
+ * positions) before using them; a failing test is counted, the first failing
+ * site is recorded as translation unit * 100000 + source line, and the access
+ * is skipped.  This reports the violations counted on the current device
+ * since the last clear (synchronizing it) and, with clear != 0, resets them.
+ * The regular library returns GP_EINVAL. */
+int gp_checked_violations(int64_t* count, int32_t* first_site, int32_t clear);
 
 /* Release cached device workspaces of the current device. */
 int gp_release_workspace(void);

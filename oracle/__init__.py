@@ -47,6 +47,9 @@ def _load():
             C.POINTER(GpOptions), C.POINTER(GpStats), C.c_void_p, C.c_void_p]
         lib.gpo_partition_prio.restype = C.c_int
         lib.gpo_partition_prio.argtypes = lib.gpo_partition.argtypes + [C.c_void_p, C.c_void_p]
+        lib.gpo_partition_prio2.restype = C.c_int
+        lib.gpo_partition_prio2.argtypes = lib.gpo_partition.argtypes + [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                                          C.c_void_p]
         lib.gpo_edge_cut.restype = C.c_int
         lib.gpo_edge_cut.argtypes = [
             C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -75,13 +78,18 @@ def _as(a, dtype):
     return None if a is None else np.ascontiguousarray(np.asarray(a), dtype=dtype)
 
 
+MPRIO_FN = C.CFUNCTYPE(C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int64)
+
+
 def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
-              options=None, trace=False, prio_levels=None):
+              options=None, trace=False, prio_levels=None, move_prio=None):
     """Full V-cycle on the CPU.  Returns (part, stats_dict, events).
 
     prio_levels: {level: int32[m_level]} matching priorities replacing the edge
     weights (the learned mode) at the levels listed; other levels use the edge
-    weights.  Fails when a listed level's entry count differs."""
+    weights.  Fails when a listed level's entry count differs.
+    move_prio: {(level, iter): int32[n_level]} move priorities replacing the
+    (gain, id) order of those label-propagation steps (learned move order)."""
     lib = _load()
     rp = _as(rowptr, np.int64)
     ci = _as(colidx, np.int32)
@@ -93,7 +101,33 @@ def partition(rowptr, colidx, k, imbalance=0.03, seed=0, vwgt=None, ewgt=None,
     opt = options if isinstance(options, GpOptions) else make_options(**(options or {}))
     col = TraceCollector() if trace else None
     tfn = C.cast(col.cfunc, C.c_void_p) if col else None
-    if prio_levels is None:
+    if move_prio is not None:
+        mheld = {(int(l), int(i)): np.ascontiguousarray(a, dtype=np.int32) for (l, i), a in move_prio.items()}
+        held = {int(l): np.ascontiguousarray(a, dtype=np.int32) for l, a in (prio_levels or {}).items()}
+        bad = []
+
+        def pcb(_user, level, m):
+            a = held.get(int(level))
+            if a is None or len(a) != int(m):
+                return None
+            return a.ctypes.data
+
+        def mcb(_user, level, it, n):
+            a = mheld.get((int(level), int(it)))
+            if a is None:
+                return None
+            if len(a) != int(n):
+                bad.append((int(level), int(it)))
+                return None
+            return a.ctypes.data
+
+        pfn, mfn = PRIO_FN(pcb), MPRIO_FN(mcb)
+        rc = lib.gpo_partition_prio2(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance),
+                                     int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st), tfn, None,
+                                     C.cast(pfn, C.c_void_p), None, C.cast(mfn, C.c_void_p), None)
+        if bad:
+            raise OracleError(-1, f"move priorities of the wrong length for (level, iter) = {bad}")
+    elif prio_levels is None:
         rc = lib.gpo_partition(n, i64p(rp), i32p(ci), i32p(vw), i32p(ew), int(k), float(imbalance),
                                int(seed) & 0xFFFFFFFFFFFFFFFF, i32p(part), C.byref(opt), C.byref(st), tfn, None)
     else:

@@ -10,7 +10,7 @@ Parameter layout (floats, row-major), H = 64 hidden, F0 = 4 input features,
 MSG = 8 message floats, ZD = 4 edge-embedding floats:
 
     W1[H, 2*F0]  b1[H]  P[MSG, H]  W2[H, H+MSG]  b2[H]  Z[ZD, H]  A[ZD]
-    beta  gamma  delta
+    beta  gamma  delta  eta
 
 Per graph (CSR, weights None = 1):
 
@@ -20,6 +20,10 @@ Per graph (CSR, weights None = 1):
     c_v  = mean_{u in N(v)} m_u
     h2_v = relu(W2 [h1_v; c_v] + b2),  z_v = Z h2_v
     t_vu = sum_j A_j z_v[j] z_u[j] + beta log2(1+w)/8 + gamma (w/wdeg_v + w/wdeg_u) + delta
+           + eta log2(1 + cn_vu)/7
+    cn_vu = popcount(sig_v & sig_u) without the bits of v and u, where the
+            128-bit signature sig_x has bit b(y) = fmix32(y * 0x9E3779B1) >> 25
+            (MurmurHash3's 32-bit finalizer) set for every neighbour y of x
     prio = clamp(rint(t * 2^bits) + 2^30, 0, 2^31 - 128)      (bits = 16 by default)
     loss = mean over directed entries of BCE-with-logits(t, label)
 
@@ -44,7 +48,8 @@ O_A = O_Z + ZD * H
 O_BETA = O_A + ZD
 O_GAMMA = O_BETA + 1
 O_DELTA = O_GAMMA + 1
-NPARAM = O_DELTA + 1
+O_ETA = O_DELTA + 1
+NPARAM = O_ETA + 1
 
 
 def bf16_round(p: np.ndarray) -> np.ndarray:
@@ -60,7 +65,7 @@ def unpack(p):
     return dict(
         W1=p[O_W1:O_B1].reshape(H, 2 * F0), b1=p[O_B1:O_P], P=p[O_P:O_W2].reshape(MSG, H),
         W2=p[O_W2:O_B2].reshape(H, H + MSG), b2=p[O_B2:O_Z], Z=p[O_Z:O_A].reshape(ZD, H),
-        A=p[O_A:O_BETA], beta=p[O_BETA], gamma=p[O_GAMMA], delta=p[O_DELTA])
+        A=p[O_A:O_BETA], beta=p[O_BETA], gamma=p[O_GAMMA], delta=p[O_DELTA], eta=p[O_ETA])
 
 
 def init_params(seed: int = 0) -> np.ndarray:
@@ -75,6 +80,41 @@ def init_params(seed: int = 0) -> np.ndarray:
     p[O_A:O_BETA] = rng.normal(0, 0.1, ZD)
     p[O_BETA] = 1.0
     return p
+
+
+def _fmix32(x):
+    x = x & 0xFFFFFFFF
+    x ^= x >> 16
+    x = (x * 0x85EBCA6B) & 0xFFFFFFFF
+    x ^= x >> 13
+    x = (x * 0xC2B2AE35) & 0xFFFFFFFF
+    x ^= x >> 16
+    return x
+
+
+def nb_bit(ids):
+    """Signature bit (0..127) of each vertex id."""
+    x = (np.asarray(ids, dtype=np.uint64) * np.uint64(0x9E3779B1)) & np.uint64(0xFFFFFFFF)
+    return (_fmix32(x) >> np.uint64(25)).astype(np.int64)
+
+
+def common_neighbours(rowptr, colidx):
+    """Per directed entry (v, u): popcount of sig_v & sig_u without the bits of v and u."""
+    rp, n, src = _rows(rowptr)
+    col = np.asarray(colidx, dtype=np.int64)
+    sig = np.zeros((n, 2), dtype=np.uint64)
+    b = nb_bit(col)
+    lo = b < 64
+    one = np.uint64(1)
+    np.bitwise_or.at(sig[:, 0], src[lo], one << b[lo].astype(np.uint64))
+    np.bitwise_or.at(sig[:, 1], src[~lo], one << (b[~lo] - 64).astype(np.uint64))
+    m = sig[src] & sig[col]
+    for ends in (src, col):
+        eb = nb_bit(ends)
+        half = (eb >= 64).astype(np.int64)
+        bit = one << (eb - 64 * half).astype(np.uint64)
+        m[np.arange(len(m)), half] &= ~bit
+    return np.bitwise_count(m).sum(1).astype(np.int64)
 
 
 def _rows(rowptr):
@@ -117,11 +157,12 @@ def forward(params, rowptr, colidx, vwgt=None, ewgt=None, level=0, keep=False):
     z = h2 @ q["Z"].T
     ft = np.log2(1 + w) / 8
     fg = w / wdeg[src] + w / wdeg[col]
-    t = (q["A"][None, :] * z[src] * z[col]).sum(1) + q["beta"] * ft + q["gamma"] * fg + q["delta"]
+    fc = np.log2(1 + common_neighbours(rp, col)) / 7
+    t = (q["A"][None, :] * z[src] * z[col]).sum(1) + q["beta"] * ft + q["gamma"] * fg + q["delta"] + q["eta"] * fc
     if not keep:
         return t
     return t, dict(src=src, col=col, inv=inv, xa=xa, pre1=pre1, h1=h1, hc=hc, pre2=pre2, h2=h2, z=z,
-                   ft=ft, fg=fg, n=n)
+                   ft=ft, fg=fg, fc=fc, n=n)
 
 
 def priorities(t, bits: int = 16):
@@ -143,6 +184,7 @@ def loss_and_grad(params, rowptr, colidx, label, vwgt=None, ewgt=None, level=0):
     g[O_BETA] = (dt * S["ft"]).sum()
     g[O_GAMMA] = (dt * S["fg"]).sum()
     g[O_DELTA] = dt.sum()
+    g[O_ETA] = (dt * S["fc"]).sum()
     dz = np.zeros((n, ZD))
     np.add.at(dz, src, dt[:, None] * q["A"][None, :] * z[col])
     np.add.at(dz, col, dt[:, None] * q["A"][None, :] * z[src])
@@ -161,4 +203,67 @@ def loss_and_grad(params, rowptr, colidx, label, vwgt=None, ewgt=None, level=0):
     dpre1 = dh1 * (S["pre1"] > 0)
     g[O_W1:O_B1] = (dpre1.T @ S["xa"]).ravel()
     g[O_B1:O_P] = dpre1.sum(0)
+    return float(loss), g
+
+
+# ---------------------------------------------------------------- move-order head
+# Parameters W1[MH, MF] b1[MH] w2[MH] b2; features of a label-propagation
+# candidate with integer gain g, degree deg, vertex weight vw at `level`:
+#   f = [sign(g) log2(1+|g|)/16, log2(1+deg)/8, log2(1+vw)/16, level/16]
+#   s = w2 . relu(W1 f + b1) + b2,   move priority = clamp(rint(s * 2^12), -2^30, 2^30)
+# trained by mean binary cross-entropy against "the candidate ends the level in
+# its proposed part".
+MH, MF = 16, 4
+MO_W1 = 0
+MO_B1 = MO_W1 + MH * MF
+MO_W2 = MO_B1 + MH
+MO_B2 = MO_W2 + MH
+MNPARAM = MO_B2 + 1
+
+
+def move_features(gain, deg, vw, level):
+    g = np.asarray(gain, dtype=np.float64)
+    mag = np.log2(1 + np.abs(g)) / 16
+    return np.stack([np.where(g < 0, -mag, mag), np.log2(1 + np.asarray(deg, dtype=np.float64)) / 8,
+                     np.log2(1 + np.asarray(vw, dtype=np.float64)) / 16,
+                     np.full(len(g), level / 16.0)], axis=1)
+
+
+def move_init_params(seed: int = 0) -> np.ndarray:
+    """He-scaled first layer; the output starts as a positive multiple of the
+    first hidden unit that copies the signed gain feature (the plain order)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MNPARAM, dtype=np.float32)
+    p[MO_W1:MO_B1] = rng.normal(0, np.sqrt(2.0 / MF), MH * MF) * 0.1
+    p[MO_W1 + 0] = 1.0                   # unit 0 <- signed log gain
+    p[MO_B1 + 0] = 0.5                   # kept positive over the gain range
+    p[MO_W2 + 0] = 4.0
+    return p
+
+
+def move_forward(params, feat):
+    p = np.asarray(params, dtype=np.float64)
+    W1 = p[MO_W1:MO_B1].reshape(MH, MF)
+    pre = feat @ W1.T + p[MO_B1:MO_W2]
+    return np.maximum(pre, 0) @ p[MO_W2:MO_B2] + p[MO_B2], pre
+
+
+def move_priorities(score):
+    return np.clip(np.rint(np.asarray(score) * 4096.0), -(1 << 30), 1 << 30).astype(np.int32)
+
+
+def move_loss_and_grad(params, feat, label):
+    p = np.asarray(params, dtype=np.float64)
+    s, pre = move_forward(p, feat)
+    y = np.asarray(label, dtype=np.float64)
+    N = max(len(s), 1)
+    loss = (np.maximum(s, 0) - s * y + np.log1p(np.exp(-np.abs(s)))).sum() / N
+    ds = (1 / (1 + np.exp(-s)) - y) / N
+    h = np.maximum(pre, 0)
+    g = np.zeros(MNPARAM)
+    g[MO_B2] = ds.sum()
+    g[MO_W2:MO_B2] = ds @ h
+    dh = (ds[:, None] * p[MO_W2:MO_B2][None, :]) * (pre > 0)
+    g[MO_B1:MO_W2] = dh.sum(0)
+    g[MO_W1:MO_B1] = (dh.T @ feat).ravel()
     return float(loss), g

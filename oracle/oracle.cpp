@@ -98,6 +98,10 @@ inline uint32_t loss_bucket(int32_t loss) {
 // weights.  The priorities are an input here: the oracle checks that the
 // integer decisions taken from them are the same on both sides.
 typedef const int32_t* (*prio_fn_t)(void* user, int32_t level, int64_t m);
+// Per-step move priorities (learned move order): mprio(user, level, iter, n)
+// returns one int32 per vertex for the label-propagation step `iter` of
+// `level`, or NULL for the (gain, id) order.  An input, like prio.
+typedef const int32_t* (*mprio_fn_t)(void* user, int32_t level, int32_t iter, int64_t n);
 
 struct Params {
     int32_t k;
@@ -108,6 +112,8 @@ struct Params {
     int64_t maxvw;   // coarse vertex weight cap
     prio_fn_t prio = nullptr;
     void* prio_user = nullptr;
+    mprio_fn_t mprio = nullptr;
+    void* mprio_user = nullptr;
 };
 
 void resolve_options(const gp_options* in, int64_t n, int32_t k, gp_options* o) {
@@ -463,13 +469,19 @@ void refine_level(const Graph& g, std::vector<int32_t>& part, const Params& P, i
                 const int64_t gn = cd - own;
                 if (gn >= 0 || -gn < own / P.o.lp_filter_den) { dest[v] = d; gain[v] = (int32_t)gn; }
             }
+            // afterburner order: (gain desc, id asc), or the learned move priorities
+            const int32_t* key = gain.data();
+            if (P.mprio) {
+                const int32_t* mp = P.mprio(P.mprio_user, level, it, n);
+                if (mp) key = mp;
+            }
             for (int64_t v = 0; v < n; ++v) {
                 if (dest[v] < 0) continue;
                 int64_t g2 = 0;
                 for (int64_t e = g.rp[v]; e < g.rp[v + 1]; ++e) {
                     const int32_t u = g.ci[e];
                     int32_t pu = part[u];
-                    if (dest[u] >= 0 && (gain[u] > gain[v] || (gain[u] == gain[v] && u < v))) pu = dest[u];
+                    if (dest[u] >= 0 && (key[u] > key[v] || (key[u] == key[v] && u < v))) pu = dest[u];
                     if (pu == dest[v]) g2 += g.ew[e];
                     else if (pu == part[v]) g2 -= g.ew[e];
                 }
@@ -641,11 +653,12 @@ int gpo_default_options(gp_options* o) {
 
 int64_t gpo_compute_lmax(int64_t W, int32_t k, float imbalance) { return compute_lmax(W, k, imbalance); }
 
-int gpo_partition_prio(int64_t n, const int64_t* rowptr, const int32_t* colidx,
-                       const int32_t* vwgt, const int32_t* ewgt, int32_t k,
-                       float imbalance, uint64_t seed, int32_t* part_out,
-                       const gp_options* opt, gp_stats* stats,
-                       gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user);
+int gpo_partition_prio2(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                        const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                        float imbalance, uint64_t seed, int32_t* part_out,
+                        const gp_options* opt, gp_stats* stats,
+                        gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user,
+                        mprio_fn_t mprio, void* mprio_user);
 
 // Full V-cycle on the CPU.  Same signature and semantics as gp_partition_ex.
 int gpo_partition(int64_t n, const int64_t* rowptr, const int32_t* colidx,
@@ -653,8 +666,8 @@ int gpo_partition(int64_t n, const int64_t* rowptr, const int32_t* colidx,
                   float imbalance, uint64_t seed, int32_t* part_out,
                   const gp_options* opt, gp_stats* stats,
                   gp_trace_fn trace, void* trace_user) {
-    return gpo_partition_prio(n, rowptr, colidx, vwgt, ewgt, k, imbalance, seed, part_out, opt, stats, trace,
-                              trace_user, nullptr, nullptr);
+    return gpo_partition_prio2(n, rowptr, colidx, vwgt, ewgt, k, imbalance, seed, part_out, opt, stats, trace,
+                               trace_user, nullptr, nullptr, nullptr, nullptr);
 }
 
 // Same, with per-level matching priorities supplied by prio (learned mode).
@@ -663,6 +676,17 @@ int gpo_partition_prio(int64_t n, const int64_t* rowptr, const int32_t* colidx,
                        float imbalance, uint64_t seed, int32_t* part_out,
                        const gp_options* opt, gp_stats* stats,
                        gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user) {
+    return gpo_partition_prio2(n, rowptr, colidx, vwgt, ewgt, k, imbalance, seed, part_out, opt, stats, trace,
+                               trace_user, prio, prio_user, nullptr, nullptr);
+}
+
+// Same, plus per-step move priorities supplied by mprio (learned move order).
+int gpo_partition_prio2(int64_t n, const int64_t* rowptr, const int32_t* colidx,
+                        const int32_t* vwgt, const int32_t* ewgt, int32_t k,
+                        float imbalance, uint64_t seed, int32_t* part_out,
+                        const gp_options* opt, gp_stats* stats,
+                        gp_trace_fn trace, void* trace_user, prio_fn_t prio, void* prio_user,
+                        mprio_fn_t mprio, void* mprio_user) {
     g_err.clear();
     if (n < 0) return fail(GP_EINVAL, "n must be >= 0");
     if (k < 1 || k > GP_MAX_K) return fail(GP_EINVAL, "k must be in [1, " + std::to_string(GP_MAX_K) + "]");
@@ -690,6 +714,7 @@ int gpo_partition_prio(int64_t n, const int64_t* rowptr, const int32_t* colidx,
     }
     P.k = k; P.seed = seed;
     P.prio = prio; P.prio_user = prio_user;
+    P.mprio = mprio; P.mprio_user = mprio_user;
     P.W = 0;
     for (int64_t v = 0; v < n; ++v) P.W += lv[0].vw[v];
     P.Lmax = compute_lmax(P.W, k, imbalance);

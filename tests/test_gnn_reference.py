@@ -59,3 +59,21 @@ def test_priority_quantisation():
     q = R.priorities(t)
     assert list(q[:3]) == [1 << 30, (1 << 30) + 65536, (1 << 30) - 65536]
     assert q[3] == 2147483520 and q[4] == 0
+
+
+def test_move_head_gradient_central_differences():
+    """The float64 move-order head: analytic gradient against central differences."""
+    from oracle import gnn_ref as R
+    rng = np.random.default_rng(3)
+    n = 400
+    feat = R.move_features(rng.integers(-300, 300, n), rng.integers(1, 200, n), rng.integers(1, 9, n), 3)
+    label = (rng.random(n) < 0.4).astype(np.uint8)
+    p = R.move_init_params(2).astype(np.float64) + rng.normal(0, 0.2, R.MNPARAM)
+    _, g = R.move_loss_and_grad(p, feat, label)
+    h = 1e-6
+    for i in range(R.MNPARAM):
+        q1, q2 = p.copy(), p.copy()
+        q1[i] += h
+        q2[i] -= h
+        num = (R.move_loss_and_grad(q1, feat, label)[0] - R.move_loss_and_grad(q2, feat, label)[0]) / (2 * h)
+        assert abs(num - g[i]) <= 1e-6 + 1e-4 * abs(num), (i, num, g[i])

@@ -18,7 +18,7 @@ import torch
 
 from thegraphpartitioning_b200 import graphs
 from thegraphpartitioning_b200 import learned
-from thegraphpartitioning_b200._abi import GP_TR_PRIO
+from thegraphpartitioning_b200._abi import GP_TR_PRIO, GP_TR_MOVE_PRIO
 from helpers import compare_traces, to_np, weighted
 
 pytestmark = pytest.mark.gpu
@@ -33,6 +33,7 @@ def _params(seed):
     p[learned.O_B2:learned.O_Z] = rng.normal(0, 0.3, learned.H)
     p[learned.O_BETA + 1] = 0.4   # gamma
     p[learned.O_BETA + 2] = -0.2  # delta
+    p[learned.O_ETA] = 0.7        # common-neighbour coefficient
     return p
 
 
@@ -207,3 +208,64 @@ def test_learned_api_rejects_invalid(gp, cuda):
     # still usable
     p, st, rep, _ = gp.partition_learned(rp, ci, 4, model, fallback=True)
     assert st["cut"] == gp.edge_cut(rp, ci, p, 4)[0]
+
+
+def test_move_head_matches_reference(gp, cuda):
+    """Move-order head: the device features, scores, priorities and gradient
+    against the float64 reference (same BF16-rounded parameters), and Adam
+    steps on the device lower the loss."""
+    from oracle import gnn_ref
+    rng = np.random.default_rng(11)
+    n = 6000
+    rp = np.concatenate([[0], np.cumsum(rng.integers(0, 300, n))]).astype(np.int64)
+    dest = rng.integers(-1, 8, n).astype(np.int32)
+    gain = rng.integers(-3000, 3000, n).astype(np.int32)
+    vw = rng.integers(1, 60, n).astype(np.int32)
+    feat = gp.GNN.move_features(_dev(rp, cuda), _dev(dest, cuda), _dev(gain, cuda), _dev(vw, cuda), level=3)
+    fref = gnn_ref.move_features(gain, np.diff(rp), vw, 3)
+    fref[dest < 0] = 0.0
+    f = feat.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(f - fref) <= 1e-6 + 1e-6 * np.abs(fref))
+    p = (gnn_ref.move_init_params(4) + rng.normal(0, 0.3, gnn_ref.MNPARAM)).astype(np.float32)
+    model = gp.GNN(learned.init_params(0))
+    model.set_move_params(p)
+    assert np.array_equal(model.get_move_params(), p)
+    score, prio = model.move_scores(feat)
+    sref, _ = gnn_ref.move_forward(gnn_ref.bf16_round(p), f)
+    sc = score.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(sc - sref) <= ATOL + RTOL * np.abs(sref))
+    assert np.all(np.abs(prio.cpu().numpy().astype(np.int64) - gnn_ref.move_priorities(sref))
+                  <= 1 + 4096 * (ATOL + RTOL * np.abs(sref)))
+    label = (rng.random(n) < 1 / (1 + np.exp(-f[:, 0] * 8))).astype(np.uint8)
+    loss, g = model.move_grad(feat, _dev(label, cuda))
+    loss_ref, g_ref = gnn_ref.move_loss_and_grad(gnn_ref.bf16_round(p), f, label)
+    assert abs(loss - loss_ref) <= 1e-5 + 1e-5 * abs(loss_ref)
+    assert np.linalg.norm(g - g_ref) <= 2e-3 * np.linalg.norm(g_ref)
+    for _ in range(60):
+        model.move_train_step(feat, _dev(label, cuda), lr=1e-2)
+    assert model.move_grad(feat, _dev(label, cuda))[0] < loss
+    model.set_move_params(None)
+    assert model.get_move_params() is None
+
+
+def test_learned_vcycle_with_move_head_matches_oracle(oracle_mod, gp, cuda):
+    """With a move-order head the afterburner orders candidates by the head's
+    priorities; the oracle, given the GPU's matching and move priorities,
+    reproduces every event of the learned run."""
+    from oracle import gnn_ref
+    rng = np.random.default_rng(5)
+    for g, k, seed in ((graphs.rmat(13, seed=23)[:2], 16, 3), (graphs.grid2d(70, 60), 6, 4)):
+        rp, ci = to_np(*g)
+        model = gp.GNN(_params(3), prio_bits=10)
+        model.set_move_params(gnn_ref.move_init_params(5) + rng.normal(0, 0.3, gnn_ref.MNPARAM).astype(np.float32))
+        part, st, rep, ev = gp.partition_learned(_dev(rp, cuda), _dev(ci, cuda), k, model, 0.03, seed,
+                                                 fallback=False, trace=True)
+        prio = {e["level"]: e["a0"] for e in ev if e["kind"] == GP_TR_PRIO}
+        mprio = {(e["level"], e["iter"]): e["a0"] for e in ev if e["kind"] == GP_TR_MOVE_PRIO}
+        assert prio and mprio and rep["kept_learned"] == 1
+        ev_gpu = [e for e in ev if e["kind"] not in (GP_TR_PRIO, GP_TR_MOVE_PRIO)]
+        p_ref, s_ref, ev_ref = oracle_mod.partition(rp, ci, k, 0.03, seed, trace=True, prio_levels=prio,
+                                                    move_prio=mprio)
+        compare_traces(ev_ref, ev_gpu)
+        assert np.array_equal(p_ref, part.cpu().numpy())
+        assert s_ref["cut"] == st["cut"]

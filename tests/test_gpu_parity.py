@@ -40,6 +40,10 @@ def _cases():
     yield "chunglu_k8_mixed", graphs.chung_lu(12000, 40000, seed=2), 8, 0.03, None, {"small_level_n": 3000}
     yield "er_k64_cta", graphs.erdos_renyi(16000, 8.0, seed=8), 64, 0.03, None, {"small_level_n": 16384}
     yield "rmat12_k16_ctas2", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"ctas_per_sm": 2}
+    # degree-bucket threshold and CTA piece length (autotuner knobs): most rows
+    # scanned by whole CTAs, long rows split into many pieces
+    yield "rmat12_k16_heavy64", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"heavy_deg": 64, "item_len": 96}
+    yield "weighted_k5_heavy64", graphs.grid2d(40, 50), 5, 0.05, "w", {"heavy_deg": 64, "small_level_n": 1200}
     # a longer refinement patience (more label-propagation / rebalancing cycles per level),
     # in the multi-kernel loop and in the one-block level loop
     yield "rmat12_k16_patience12", graphs.rmat(12, seed=1)[:2], 16, 0.03, None, {"refine_patience": 12}

@@ -23,7 +23,10 @@ from ._abi import (
 )
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgp_b200.so")
+# THEGRAPHPARTITIONING_CHECKED=1 selects the bounds-checked build of the same
+# sources (device-side index checks; gp_checked_violations reports them)
+CHECKED = os.environ.get("THEGRAPHPARTITIONING_CHECKED", "") == "1"
+LIB_PATH = os.path.join(HERE, "libgp_b200_checked.so" if CHECKED else "libgp_b200.so")
 CLI_PATH = os.path.join(HERE, "bin", "gpu_part")
 _lib = None
 
@@ -94,12 +97,27 @@ def lib():
     L.gp_gnn_train_step_device.restype = C.c_int
     L.gp_gnn_train_step_device.argtypes = [VP, C.c_int32, P64, PP64, PP32, PP32, PP32, P32, C.POINTER(VP),
                                            C.c_float, VP, C.POINTER(C.c_float)]
+    L.gp_gnn_move_num_params.restype = C.c_int
+    L.gp_gnn_set_move_params.restype = C.c_int
+    L.gp_gnn_set_move_params.argtypes = [VP, C.POINTER(C.c_float), C.c_int32]
+    L.gp_gnn_get_move_params.restype = C.c_int
+    L.gp_gnn_get_move_params.argtypes = [VP, C.POINTER(C.c_float), C.c_int32]
+    L.gp_gnn_move_features_device.restype = C.c_int
+    L.gp_gnn_move_features_device.argtypes = [C.c_int64, VP, VP, VP, VP, C.c_int32, VP, VP]
+    L.gp_gnn_move_scores_device.restype = C.c_int
+    L.gp_gnn_move_scores_device.argtypes = [VP, C.c_int64, VP, VP, VP, VP]
+    L.gp_gnn_move_grad_device.restype = C.c_int
+    L.gp_gnn_move_grad_device.argtypes = [VP, C.c_int64, VP, VP, VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.gp_gnn_move_train_step_device.restype = C.c_int
+    L.gp_gnn_move_train_step_device.argtypes = [VP, C.c_int64, VP, VP, C.c_float, VP, C.POINTER(C.c_float)]
     L.gp_partition_learned_device.restype = C.c_int
     L.gp_partition_learned_device.argtypes = [C.c_int64, VP, VP, VP, VP, C.c_int32, C.c_float, C.c_uint64, VP, VP,
                                               C.POINTER(GpOptions), C.POINTER(GpStats), VP, C.c_int32,
                                               C.POINTER(GpLearnedReport), VP, VP]
     L.gp_default_options.restype = C.c_int
     L.gp_default_options.argtypes = [C.POINTER(GpOptions)]
+    L.gp_checked_violations.restype = C.c_int
+    L.gp_checked_violations.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.c_int32]
     L.gp_release_workspace.restype = C.c_int
     L.gp_last_error.restype = C.c_char_p
     L.gp_version.restype = C.c_char_p
@@ -290,18 +308,98 @@ class GNN:
         _check(lib().gp_gnn_get_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p)))
         return p
 
+    # ---- move-order head (learned order of the label-propagation afterburner)
+    @staticmethod
+    def move_num_params() -> int:
+        return int(lib().gp_gnn_move_num_params())
+
+    def set_move_params(self, params) -> None:
+        """Install the move-order head (None removes it)."""
+        if params is None:
+            _check(lib().gp_gnn_set_move_params(self._h, None, 0))
+            return
+        p = np.ascontiguousarray(np.asarray(params), dtype=np.float32)
+        _check(lib().gp_gnn_set_move_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p)))
+
+    def get_move_params(self):
+        """The head's parameters, or None when the model has none."""
+        p = np.zeros(self.move_num_params(), dtype=np.float32)
+        rc = lib().gp_gnn_get_move_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p))
+        return p if rc == 0 else None
+
+    @staticmethod
+    def move_features(rowptr, dest, gain, vwgt=None, level: int = 0, stream=None):
+        """float32[n, 4] CUDA tensor: the head's features of every candidate (dest >= 0)."""
+        import torch
+        n = rowptr.numel() - 1
+        feat = torch.empty((max(n, 0), 4), dtype=torch.float32, device=rowptr.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(rowptr.device).cuda_stream
+        _check(lib().gp_gnn_move_features_device(n, _ptr(rowptr), _ptr(vwgt), _ptr(dest), _ptr(gain), int(level),
+                                                 C.c_void_p(stream), _ptr(feat)))
+        return feat
+
+    def move_scores(self, feat, stream=None):
+        """(score float32, move priority int32) CUDA tensors of feature rows."""
+        import torch
+        ns = feat.shape[0]
+        score = torch.empty(ns, dtype=torch.float32, device=feat.device)
+        prio = torch.empty(ns, dtype=torch.int32, device=feat.device)
+        if stream is None:
+            stream = torch.cuda.current_stream(feat.device).cuda_stream
+        _check(lib().gp_gnn_move_scores_device(self._h, ns, _ptr(feat), C.c_void_p(stream), _ptr(score), _ptr(prio)))
+        return score, prio
+
+    def move_grad(self, feat, label, stream=None):
+        """(mean BCE, gradient float32[move_num_params]) of labelled feature rows."""
+        import torch
+        loss = C.c_float(0)
+        g = np.zeros(self.move_num_params(), dtype=np.float32)
+        if stream is None:
+            stream = torch.cuda.current_stream(feat.device).cuda_stream
+        _check(lib().gp_gnn_move_grad_device(self._h, feat.shape[0], _ptr(feat), _ptr(label), C.c_void_p(stream),
+                                             C.byref(loss), g.ctypes.data_as(C.POINTER(C.c_float))))
+        return float(loss.value), g
+
+    def move_train_step(self, feat, label, lr: float = 1e-2, stream=None) -> float:
+        """One Adam step of the head; returns the loss before it."""
+        import torch
+        loss = C.c_float(0)
+        if stream is None:
+            stream = torch.cuda.current_stream(feat.device).cuda_stream
+        _check(lib().gp_gnn_move_train_step_device(self._h, feat.shape[0], _ptr(feat), _ptr(label), float(lr),
+                                                   C.c_void_p(stream), C.byref(loss)))
+        return float(loss.value)
+
     def save(self, path: str) -> None:
-        """params (float32), prio_bits and max_level in one .npz file."""
+        """params (float32), prio_bits, max_level and the move-order head (when
+        present) in one .npz file."""
+        extra = {}
+        mp = self.get_move_params()
+        if mp is not None:
+            extra["move_params"] = mp
         with open(path, "wb") as f:
             np.savez(f, params=self.get_params(), prio_bits=np.int32(self.prio_bits),
-                     max_level=np.int32(self.max_level))
+                     max_level=np.int32(self.max_level), **extra)
 
     @classmethod
     def load(cls, path: str) -> "GNN":
         z = np.load(path)
         if isinstance(z, np.ndarray):        # bare parameter array
-            return cls(z)
-        return cls(z["params"], int(z["prio_bits"]), int(z["max_level"]) if "max_level" in z.files else -1)
+            return cls(cls._fit(z))
+        m = cls(cls._fit(z["params"]), int(z["prio_bits"]), int(z["max_level"]) if "max_level" in z.files else -1)
+        if "move_params" in z.files:
+            m.set_move_params(z["move_params"])
+        return m
+
+    @classmethod
+    def _fit(cls, p):
+        """Parameters saved before the common-neighbour coefficient (the last
+        one) existed get it as 0, which reproduces their scores."""
+        p = np.asarray(p, dtype=np.float32)
+        if len(p) == cls.num_params() - 1:
+            p = np.concatenate([p, np.zeros(1, np.float32)])
+        return p
 
     def forward(self, rowptr, colidx, vwgt=None, ewgt=None, level: int = 0, stream=None):
         """(priority int32[m], logit float32[m]) CUDA tensors of one graph."""
@@ -400,6 +498,14 @@ def default_options() -> GpOptions:
     o = GpOptions()
     _check(lib().gp_default_options(C.byref(o)))
     return o
+
+
+def checked_violations(clear: bool = True):
+    """Bounds-checked build only: (violations counted, first failing site as
+    translation unit * 100000 + line, or -1) since the last clear."""
+    cnt, site = C.c_int64(0), C.c_int32(0)
+    _check(lib().gp_checked_violations(C.byref(cnt), C.byref(site), 1 if clear else 0))
+    return int(cnt.value), int(site.value)
 
 
 def release_workspace() -> None:

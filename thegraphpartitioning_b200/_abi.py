@@ -24,6 +24,7 @@ GP_TR_INITPART = 3
 GP_TR_REFINE_ITER = 4
 GP_TR_LEVEL_DONE = 5
 GP_TR_PRIO = 6
+GP_TR_MOVE_PRIO = 7
 
 ERROR_NAMES = {
     GP_EINVAL: "GP_EINVAL",
@@ -50,7 +51,8 @@ class GpOptions(C.Structure):
         ("profile", C.c_int32),
         ("small_level_n", C.c_int32),
         ("ctas_per_sm", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("heavy_deg", C.c_int32),
+        ("item_len", C.c_int32),
     ]
 
 
@@ -161,6 +163,8 @@ def decode_event(ev: GpTraceEvent) -> dict:
         d["vwgt"] = _arr(ev.vwgt, n, np.int32)
     elif ev.kind == GP_TR_PRIO:
         d["a0"] = _arr(ev.a0, int(ev.m), np.int32)
+    elif ev.kind == GP_TR_MOVE_PRIO:
+        d["a0"] = _arr(ev.a0, n, np.int32)
     else:
         for name in ("a0", "a1", "a2"):
             d[name] = _arr(getattr(ev, name), n, np.int32)

@@ -7,6 +7,7 @@
 // Differences by design: every step runs on the device (no gpmetis process,
 // no per-element host partCount rebuild), errors are returned instead of
 // exit(), and all integer results are deterministic for a given seed.
+#define GP_TU_ID 5   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 #include <mutex>
@@ -16,6 +17,15 @@
 namespace gp {
 
 thread_local std::string t_err;
+
+#ifdef GP_CHECKED
+// the per-translation-unit violation counters of the bounds-checked build
+static std::vector<chk_fetch_fn>& chk_fetchers() {
+    static std::vector<chk_fetch_fn> v;
+    return v;
+}
+void chk_register(chk_fetch_fn f) { chk_fetchers().push_back(f); }
+#endif
 
 // ---------------------------------------------------------------- device state
 struct DevState {
@@ -212,160 +222,186 @@ static std::vector<T> to_host(Ctx& c, const T* d, int64_t count) {
 }
 
 // ---------------------------------------------------------------- V-cycle
-struct Timer {
-    cudaEvent_t e[8];
-    Timer() { for (auto& x : e) cudaEventCreate(&x); }
-    ~Timer() { for (auto& x : e) cudaEventDestroy(x); }
-    double ms(int a, int b) { float t = 0; cudaEventElapsedTime(&t, e[a], e[b]); return t; }
-};
 
-void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
-                int32_t* d_out, gp_stats* st, const Tracer& tr, const gp_gnn* gnn) {
-    Params P;
+// Phase 1: validation, coarsening, refinement buffers and the initial
+// partition.  Everything the later phases need stays in S (hierarchy and
+// buffers in c.keep, which must outlive the V-cycle).
+void vc_begin(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
+              VState& S, const Tracer& tr, const gp_gnn* gnn) {
+    Params& P = S.P;
     P.gnn = gnn;
     resolve_options(opt, k, &P.o);
     P.k = k; P.seed = seed; P.imbalance = imbalance;
     c.ctas_per_sm = P.o.ctas_per_sm;
-    Timer tm;
+    Timer& tm = S.tm;
     c.profile = P.o.profile > 0;
     if (c.profile) { c.ev_a = tm.e[6]; c.ev_b = tm.e[7]; }
     GP_CUDA(cudaEventRecord(tm.e[0], c.s));
     P.W = validate(c, g0, P.o.check_input);
     P.Lmax = compute_lmax(P.W, k, imbalance);
     P.maxvw = std::max<int64_t>(1, (3 * P.W) / (2 * (int64_t)P.o.coarsen_to));
+    S.g0 = g0;
     const int64_t n0 = g0.n;
-    std::vector<Level> lv(1);
+    std::vector<Level>& lv = S.lv;
+    lv.assign(1, Level());
     lv[0].g = g0;
-    int best_trial = -1, iters = 0;
-    double ms_coarsen = 0, ms_init = 0, ms_refine = 0;
+    S.best_trial = -1; S.iters = 0;
     if (k == 1) {
-        memset_async(c, d_out, 0, sizeof(int32_t) * n0);
+        S.L = 0;
+        S.refined_to = 0;
         GP_CUDA(cudaEventRecord(tm.e[1], c.s));
         GP_CUDA(cudaEventRecord(tm.e[2], c.s));
-        GP_CUDA(cudaEventRecord(tm.e[3], c.s));
-    } else {
-        build_heavy(c, lv[0]);
-        // ---- coarsening
-        while (lv.back().g.n > P.o.coarsen_to && (int)lv.size() < 64) {
-            const int level = (int)lv.size() - 1;
-            auto mk = c.tmp->save();
-            int32_t* match = c.tmp_alloc<int32_t>(lv.back().g.n);
-            int32_t* prio = nullptr;
-            const bool scored = P.gnn && gnn_scores_level(P.gnn, level);
-            if (scored) {
-                prio = c.tmp_alloc<int32_t>(lv.back().g.m);
-                GP_CUDA(cudaEventRecord(tm.e[4], c.s));
-                gnn_level_priorities(c, P.gnn, lv.back(), level, prio);
-                GP_CUDA(cudaEventRecord(tm.e[5], c.s));
-                if (tr.on()) {
-                    auto hp = to_host(c, prio, lv.back().g.m);
-                    gp_trace_event ev; memset(&ev, 0, sizeof ev);
-                    ev.kind = GP_TR_PRIO; ev.level = level; ev.n = lv.back().g.n; ev.m = lv.back().g.m;
-                    ev.a0 = hp.data();
-                    tr.emit(ev);
-                }
-            }
-            int rounds = 0;
-            const int64_t pairs = match_level(c, lv.back(), level, P, match, &rounds, prio);
-            if (scored) c.ms_gnn += tm.ms(4, 5);   // match_level has synchronized the stream
-            const int64_t n = lv.back().g.n;
+        S.take(c);
+        return;
+    }
+    lv[0].heavy_deg = P.o.heavy_deg;
+    lv[0].item_len = P.o.item_len;
+    build_heavy(c, lv[0]);
+    // ---- coarsening
+    while (lv.back().g.n > P.o.coarsen_to && (int)lv.size() < 64) {
+        const int level = (int)lv.size() - 1;
+        auto mk = c.tmp->save();
+        int32_t* match = c.tmp_alloc<int32_t>(lv.back().g.n);
+        int32_t* prio = nullptr;
+        const bool scored = P.gnn && gnn_scores_level(P.gnn, level);
+        if (scored) {
+            prio = c.tmp_alloc<int32_t>(lv.back().g.m);
+            GP_CUDA(cudaEventRecord(tm.e[4], c.s));
+            gnn_level_priorities(c, P.gnn, lv.back(), level, prio);
+            GP_CUDA(cudaEventRecord(tm.e[5], c.s));
             if (tr.on()) {
-                auto h = to_host(c, match, n);
+                auto hp = to_host(c, prio, lv.back().g.m);
                 gp_trace_event ev; memset(&ev, 0, sizeof ev);
-                ev.kind = GP_TR_MATCH; ev.level = level; ev.iter = rounds; ev.n = n; ev.m = lv.back().g.m;
-                ev.count = pairs; ev.a0 = h.data();
+                ev.kind = GP_TR_PRIO; ev.level = level; ev.n = lv.back().g.n; ev.m = lv.back().g.m;
+                ev.a0 = hp.data();
                 tr.emit(ev);
             }
-            if (20 * (n - pairs) > 19 * n) { c.tmp->restore(mk); break; }
-            Level cl;
-            contract_level(c, lv.back(), cl, match);
-            c.tmp->restore(mk);
-            if (tr.on()) {
-                auto cm = to_host(c, lv.back().cmap, n);
-                auto rp = to_host(c, cl.g.rp, cl.g.n + 1);
-                auto ci = to_host(c, cl.g.ci, cl.g.m);
-                auto ew = to_host(c, cl.g.ew, cl.g.m);
-                auto vw = to_host(c, cl.g.vw, cl.g.n);
-                gp_trace_event ev; memset(&ev, 0, sizeof ev);
-                ev.kind = GP_TR_CONTRACT; ev.level = level; ev.n = cl.g.n; ev.m = cl.g.m;
-                ev.a0 = cm.data(); ev.rowptr = rp.data(); ev.colidx = ci.data(); ev.ewgt = ew.data(); ev.vwgt = vw.data();
-                tr.emit(ev);
-            }
-            build_heavy(c, cl);
-            lv.push_back(cl);
         }
-        GP_CUDA(cudaEventRecord(tm.e[1], c.s));
-        // ---- refinement buffers (finest size)
-        RefineBufs B;
-        B.part = c.keep_alloc<int32_t>(n0);
-        B.part_next = c.keep_alloc<int32_t>(n0);
-        B.best = c.keep_alloc<int32_t>(n0);
-        B.pc = c.keep_alloc<uint16_t>(n0);
-        B.pc_next = c.keep_alloc<uint16_t>(n0);
-        B.dest = c.keep_alloc<int32_t>(n0);
-        B.gain = c.keep_alloc<int32_t>(n0);
-        B.lock = c.keep_alloc<uint8_t>(n0);
-        B.lock_next = c.keep_alloc<uint8_t>(n0);
-        B.pw = c.keep_alloc<int64_t>(k);
-        B.best_pw = c.keep_alloc<int64_t>(k);
-        B.status = c.keep_alloc<int64_t>(S_NSLOTS);
-        for (int b = 0; b < 3; ++b) B.clist[b] = c.keep_alloc<int32_t>(n0);
-        int64_t hmax = 1;
-        for (const Level& l : lv) hmax = std::max(hmax, l.nheavy);
-        B.hhist = c.keep_alloc<int32_t>(hmax * k);
-        B.hsum = c.keep_alloc<int64_t>(2 * hmax);
-        B.hdone = c.keep_alloc<int32_t>(hmax);
-        memset_async(c, B.hhist, 0, sizeof(int32_t) * hmax * k);
-        memset_async(c, B.hsum, 0, sizeof(int64_t) * 2 * hmax);
-        memset_async(c, B.hdone, 0, sizeof(int32_t) * hmax);
-        B.ckeys = c.keep_alloc<uint64_t>(n0);
-        B.cvals = c.keep_alloc<int32_t>(n0);
-        B.ckeys2 = c.keep_alloc<uint64_t>(n0);
-        B.cvals2 = c.keep_alloc<int32_t>(n0);
-        // ---- initial partition
-        const int L = (int)lv.size() - 1;
-        best_trial = initial_partition(c, lv[L], P, B.part);
-        part_weights(c, lv[L].g, B.part, k, B.pw);
+        int rounds = 0;
+        const int64_t pairs = match_level(c, lv.back(), level, P, match, &rounds, prio);
+        if (scored) c.ms_gnn += tm.ms(4, 5);   // match_level has synchronized the stream
+        const int64_t n = lv.back().g.n;
         if (tr.on()) {
-            int64_t* d_c = c.tmp_alloc<int64_t>(1);
-            cut_and_weights(c, lv[L].g, B.part, k, d_c, nullptr);
-            auto cut2 = to_host(c, d_c, 1);
-            auto pw = to_host(c, B.pw, k);
-            auto hp = to_host(c, B.part, lv[L].g.n);
+            auto h = to_host(c, match, n);
             gp_trace_event ev; memset(&ev, 0, sizeof ev);
-            ev.kind = GP_TR_INITPART; ev.level = L; ev.iter = best_trial; ev.n = lv[L].g.n; ev.m = lv[L].g.m;
-            ev.cut = cut2[0] / 2; ev.maxpw = *std::max_element(pw.begin(), pw.begin() + k); ev.a0 = hp.data();
+            ev.kind = GP_TR_MATCH; ev.level = level; ev.iter = rounds; ev.n = n; ev.m = lv.back().g.m;
+            ev.count = pairs; ev.a0 = h.data();
             tr.emit(ev);
         }
-        GP_CUDA(cudaEventRecord(tm.e[2], c.s));
-        // ---- uncoarsening
-        for (int l = L; l >= 0; --l) {
-            if (l < L) {
-                project(c, lv[l], B.part, B.part_next);
-                std::swap(B.part, B.part_next);
-            }
-            iters += refine_level(c, lv[l], P, B, l, tr);
-            if (tr.on()) {
-                int64_t* d_c = c.tmp_alloc<int64_t>(1);
-                cut_and_weights(c, lv[l].g, B.part, k, d_c, nullptr);
-                auto cut2 = to_host(c, d_c, 1);
-                auto pw = to_host(c, B.pw, k);
-                auto hp = to_host(c, B.part, lv[l].g.n);
-                gp_trace_event ev; memset(&ev, 0, sizeof ev);
-                ev.kind = GP_TR_LEVEL_DONE; ev.level = l; ev.n = lv[l].g.n; ev.m = lv[l].g.m;
-                ev.cut = cut2[0] / 2; ev.maxpw = *std::max_element(pw.begin(), pw.begin() + k); ev.a0 = hp.data();
-                tr.emit(ev);
-            }
+        if (20 * (n - pairs) > 19 * n) { c.tmp->restore(mk); break; }
+        Level cl;
+        contract_level(c, lv.back(), cl, match);
+        c.tmp->restore(mk);
+        if (tr.on()) {
+            auto cm = to_host(c, lv.back().cmap, n);
+            auto rp = to_host(c, cl.g.rp, cl.g.n + 1);
+            auto ci = to_host(c, cl.g.ci, cl.g.m);
+            auto ew = to_host(c, cl.g.ew, cl.g.m);
+            auto vw = to_host(c, cl.g.vw, cl.g.n);
+            gp_trace_event ev; memset(&ev, 0, sizeof ev);
+            ev.kind = GP_TR_CONTRACT; ev.level = level; ev.n = cl.g.n; ev.m = cl.g.m;
+            ev.a0 = cm.data(); ev.rowptr = rp.data(); ev.colidx = ci.data(); ev.ewgt = ew.data(); ev.vwgt = vw.data();
+            tr.emit(ev);
         }
-        GP_CUDA(cudaMemcpyAsync(d_out, B.part, sizeof(int32_t) * n0, cudaMemcpyDeviceToDevice, c.s));
-        GP_CUDA(cudaEventRecord(tm.e[3], c.s));
+        cl.heavy_deg = P.o.heavy_deg;
+        cl.item_len = P.o.item_len;
+        build_heavy(c, cl);
+        lv.push_back(cl);
     }
-    // ---- exact result record
+    GP_CUDA(cudaEventRecord(tm.e[1], c.s));
+    // ---- refinement buffers (finest size)
+    RefineBufs& B = S.B;
+    B.part = c.keep_alloc<int32_t>(n0);
+    B.part_next = c.keep_alloc<int32_t>(n0);
+    B.best = c.keep_alloc<int32_t>(n0);
+    B.pc = c.keep_alloc<uint16_t>(n0);
+    B.pc_next = c.keep_alloc<uint16_t>(n0);
+    B.dest = c.keep_alloc<int32_t>(n0);
+    B.gain = c.keep_alloc<int32_t>(n0);
+    B.mp = P.gnn && gnn_has_move_head(P.gnn) ? c.keep_alloc<int32_t>(n0) : nullptr;
+    B.lock = c.keep_alloc<uint8_t>(n0);
+    B.lock_next = c.keep_alloc<uint8_t>(n0);
+    B.pw = c.keep_alloc<int64_t>(k);
+    B.best_pw = c.keep_alloc<int64_t>(k);
+    B.status = c.keep_alloc<int64_t>(S_NSLOTS);
+    for (int b = 0; b < 3; ++b) B.clist[b] = c.keep_alloc<int32_t>(n0);
+    int64_t hmax = 1;
+    for (const Level& l : lv) hmax = std::max(hmax, l.nheavy);
+    B.hhist = c.keep_alloc<int32_t>(hmax * k);
+    B.hsum = c.keep_alloc<int64_t>(2 * hmax);
+    B.hdone = c.keep_alloc<int32_t>(hmax);
+    memset_async(c, B.hhist, 0, sizeof(int32_t) * hmax * k);
+    memset_async(c, B.hsum, 0, sizeof(int64_t) * 2 * hmax);
+    memset_async(c, B.hdone, 0, sizeof(int32_t) * hmax);
+    B.ckeys = c.keep_alloc<uint64_t>(n0);
+    B.cvals = c.keep_alloc<int32_t>(n0);
+    B.ckeys2 = c.keep_alloc<uint64_t>(n0);
+    B.cvals2 = c.keep_alloc<int32_t>(n0);
+    // ---- initial partition
+    const int L = (int)lv.size() - 1;
+    S.L = L;
+    S.refined_to = L + 1;
+    S.best_trial = initial_partition(c, lv[L], P, B.part);
+    part_weights(c, lv[L].g, B.part, k, B.pw);
+    if (tr.on()) {
+        int64_t* d_c = c.tmp_alloc<int64_t>(1);
+        cut_and_weights(c, lv[L].g, B.part, k, d_c, nullptr);
+        auto cut2 = to_host(c, d_c, 1);
+        auto pw = to_host(c, B.pw, k);
+        auto hp = to_host(c, B.part, lv[L].g.n);
+        gp_trace_event ev; memset(&ev, 0, sizeof ev);
+        ev.kind = GP_TR_INITPART; ev.level = L; ev.iter = S.best_trial; ev.n = lv[L].g.n; ev.m = lv[L].g.m;
+        ev.cut = cut2[0] / 2; ev.maxpw = *std::max_element(pw.begin(), pw.begin() + k); ev.a0 = hp.data();
+        tr.emit(ev);
+    }
+    GP_CUDA(cudaEventRecord(tm.e[2], c.s));
+    S.take(c);
+}
+
+// Phase 2, one level at a time from the coarsest (l = S.L) to the input
+// (l = 0): projection of the coarser level's partition, then refinement.
+void vc_level(Ctx& c, VState& S, int l, const Tracer& tr) {
+    if (l != S.refined_to - 1) throw GpError(GP_EINTERNAL, "levels must be refined coarsest first");
+    const Params& P = S.P;
+    RefineBufs& B = S.B;
+    std::vector<Level>& lv = S.lv;
+    c.ctas_per_sm = P.o.ctas_per_sm;
+    c.profile = P.o.profile > 0;
+    if (c.profile) { c.ev_a = S.tm.e[6]; c.ev_b = S.tm.e[7]; }
+    if (l < S.L) {
+        project(c, lv[l], B.part, B.part_next);
+        std::swap(B.part, B.part_next);
+    }
+    S.iters += refine_level(c, lv[l], P, B, l, tr);
+    if (tr.on()) {
+        int64_t* d_c = c.tmp_alloc<int64_t>(1);
+        cut_and_weights(c, lv[l].g, B.part, P.k, d_c, nullptr);
+        auto cut2 = to_host(c, d_c, 1);
+        auto pw = to_host(c, B.pw, P.k);
+        auto hp = to_host(c, B.part, lv[l].g.n);
+        gp_trace_event ev; memset(&ev, 0, sizeof ev);
+        ev.kind = GP_TR_LEVEL_DONE; ev.level = l; ev.n = lv[l].g.n; ev.m = lv[l].g.m;
+        ev.cut = cut2[0] / 2; ev.maxpw = *std::max_element(pw.begin(), pw.begin() + P.k); ev.a0 = hp.data();
+        tr.emit(ev);
+    }
+    S.refined_to = l;
+    S.take(c);
+}
+
+// Phase 3: the result into d_out and the exact result record.
+void vc_end(Ctx& c, VState& S, int32_t* d_out, gp_stats* st) {
+    const Params& P = S.P;
+    const int32_t k = P.k;
+    const int64_t n0 = S.g0.n;
+    if (k == 1) memset_async(c, d_out, 0, sizeof(int32_t) * n0);
+    else GP_CUDA(cudaMemcpyAsync(d_out, S.B.part, sizeof(int32_t) * n0, cudaMemcpyDeviceToDevice, c.s));
+    GP_CUDA(cudaEventRecord(S.tm.e[3], c.s));
     int64_t* d_c = c.tmp_alloc<int64_t>(1);
     int64_t* d_pw = c.tmp_alloc<int64_t>(k);
-    cut_and_weights(c, g0, d_out, k, d_c, d_pw);
+    cut_and_weights(c, S.g0, d_out, k, d_c, d_pw);
     auto cut2 = to_host(c, d_c, 1);
     auto pw = to_host(c, d_pw, k);
+    S.take(c);
     if (st) {
         memset(st, 0, sizeof *st);
         st->cut = cut2[0] / 2;
@@ -373,21 +409,30 @@ void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t s
         st->total_weight = P.W;
         st->max_allowed = P.Lmax;
         st->imbalance = (double)st->max_part_weight * k / (double)P.W - 1.0;
-        st->levels = (int32_t)lv.size();
-        st->coarsest_n = (int32_t)lv.back().g.n;
-        st->best_trial = best_trial;
-        st->refine_iters = iters;
-        st->algo_bytes = c.bytes;
-        st->kernel_launches = c.launches;
-        ms_coarsen = tm.ms(0, 1); ms_init = tm.ms(1, 2); ms_refine = tm.ms(2, 3);
-        st->ms_coarsen = ms_coarsen;
-        st->ms_initial = ms_init;
-        st->ms_refine = ms_refine;
-        st->ms_total = tm.ms(0, 3);
-        st->ms_conn = c.ms_conn;
-        st->conn_launches = c.conn_launches;
-        st->conn_bytes = c.conn_bytes;
+        st->levels = (int32_t)S.lv.size();
+        st->coarsest_n = (int32_t)S.lv.back().g.n;
+        st->best_trial = S.best_trial;
+        st->refine_iters = S.iters;
+        st->algo_bytes = S.bytes;
+        st->kernel_launches = S.launches;
+        st->ms_coarsen = S.tm.ms(0, 1);
+        st->ms_initial = S.tm.ms(1, 2);
+        st->ms_refine = S.tm.ms(2, 3);
+        st->ms_total = S.tm.ms(0, 3);
+        st->ms_conn = S.ms_conn;
+        st->conn_launches = S.conn_launches;
+        st->conn_bytes = S.conn_bytes;
     }
+}
+
+void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
+                int32_t* d_out, gp_stats* st, const Tracer& tr, const gp_gnn* gnn) {
+    VState S;
+    vc_begin(c, g0, k, imbalance, seed, opt, S, tr, gnn);
+    if (k > 1)
+        for (int l = S.L; l >= 0; --l) vc_level(c, S, l, tr);
+    vc_end(c, S, d_out, st);
+    c.ms_gnn = S.ms_gnn;
 }
 
 struct CallGuard {
@@ -447,7 +492,32 @@ extern "C" {
 
 const char* gp_last_error(void) { return t_err.c_str(); }
 
-const char* gp_version(void) { return "thegraphpartitioning_b200 0.1 (sm_100a)"; }
+const char* gp_version(void) {
+#ifdef GP_CHECKED
+    return "thegraphpartitioning_b200 0.2 (sm_100a, bounds-checked)";
+#else
+    return "thegraphpartitioning_b200 0.2 (sm_100a)";
+#endif
+}
+
+int gp_checked_violations(int64_t* count, int32_t* first_site, int32_t clear) {
+    return guarded([&] {
+        if (!count || !first_site) throw GpError(GP_EINVAL, "null output");
+#ifdef GP_CHECKED
+        GP_CUDA(cudaDeviceSynchronize());
+        unsigned long long c = 0, f = 0;
+        for (chk_fetch_fn fn : chk_fetchers()) fn(&c, &f, clear != 0);
+        GP_CUDA(cudaGetLastError());
+        *count = (int64_t)c;
+        *first_site = f ? (int32_t)(f - 1) : -1;
+#else
+        (void)clear;
+        *count = -1;
+        *first_site = -1;
+        throw GpError(GP_EINVAL, "not the bounds-checked build (libgp_b200_checked.so)");
+#endif
+    });
+}
 
 int gp_default_options(gp_options* opt) {
     return guarded([&] {
@@ -505,6 +575,16 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
         if (g.m < 0) throw GpError(GP_EINVAL, "rowptr[n] must be >= 0");
         g.ci = d_colidx; g.ew = d_ewgt; g.vw = d_vwgt;
         Tracer tr; tr.fn = trace; tr.user = trace_user;
+        // the scorer's float sums follow the row layout, so the learned
+        // V-cycle keeps the default heavy-row threshold and piece length
+        gp_options lopt;
+        if (opt) lopt = *opt;
+        else { memset(&lopt, 0, sizeof lopt); lopt.version = GP_OPTIONS_VERSION; }
+        lopt.heavy_deg = 0;
+        lopt.item_len = 0;
+        // the move-order head runs in the multi-kernel refinement loop only
+        if (gnn_has_move_head(model)) lopt.small_level_n = 0;
+        opt = &lopt;
         gp_stats sl;
         c.ms_gnn = 0;
         run_vcycle(c, g, k, imbalance, seed, opt, d_part_out, &sl, tr, model);

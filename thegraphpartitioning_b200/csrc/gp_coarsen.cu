@@ -9,6 +9,7 @@
 // a NULL weight array means unit weights (the input level only).  Rows longer
 // than kHeavyDeg are handled by one CTA each (blocks [0, nheavy) of a launch);
 // all other rows by one warp each (grid-stride over the remaining blocks).
+#define GP_TU_ID 2   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 namespace gp {
@@ -16,27 +17,29 @@ namespace gp {
 // ---------------------------------------------------------------- degree buckets
 // Lists in any order (each row is processed on its own).  Appends are
 // aggregated per warp: one atomic per warp and bucket.
-__device__ __forceinline__ void warp_append(bool take, int32_t v, int32_t* list, int64_t* count) {
+__device__ __forceinline__ void warp_append(bool take, int32_t v, int32_t* list, int64_t* count, int64_t cap) {
     const uint32_t m = __ballot_sync(0xffffffffu, take);
     if (!m) return;
     const int lane = threadIdx.x & 31;
     unsigned long long base = 0;
     if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)count, (unsigned long long)__popc(m));
     base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (take) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+    const int64_t idx = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (take && GP_IN(idx, cap)) list[idx] = v;
 }
 
-__global__ void k_buckets(const int64_t* __restrict__ rp, int64_t n, int32_t* __restrict__ heavy,
+__global__ void k_buckets(const int64_t* __restrict__ rp, int64_t n, int32_t heavy_deg, int64_t heavy_cap,
+                          int32_t* __restrict__ heavy,
                           int32_t* __restrict__ b0, int32_t* __restrict__ b1, int32_t* __restrict__ b2,
                           int64_t* __restrict__ count) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
         const int64_t v = base + threadIdx.x;
         const int64_t d = v < n ? rp[v + 1] - rp[v] : -1;
-        warp_append(v < n && d <= kTile8, (int32_t)v, b0, &count[0]);
-        warp_append(d > kTile8 && d <= kTile32, (int32_t)v, b1, &count[1]);
-        warp_append(d > kTile32 && d <= kHeavyDeg, (int32_t)v, b2, &count[2]);
-        warp_append(d > kHeavyDeg, (int32_t)v, heavy, &count[3]);
+        warp_append(v < n && d <= kTile8, (int32_t)v, b0, &count[0], n);
+        warp_append(d > kTile8 && d <= kTile32, (int32_t)v, b1, &count[1], n);
+        warp_append(d > kTile32 && d <= heavy_deg, (int32_t)v, b2, &count[2], n);
+        warp_append(d > heavy_deg, (int32_t)v, heavy, &count[3], heavy_cap);
     }
 }
 
@@ -69,9 +72,10 @@ void build_heavy(Ctx& c, Level& L) {
     auto mk = c.tmp->save();
     int64_t* d_cnt = c.tmp_alloc<int64_t>(4);
     memset_async(c, d_cnt, 0, 4 * sizeof(int64_t));
-    L.heavy = c.keep_alloc<int32_t>(std::max<int64_t>(1, L.g.m / kHeavyDeg + 1));
+    const int64_t heavy_cap = std::max<int64_t>(1, L.g.m / L.heavy_deg + 1);
+    L.heavy = c.keep_alloc<int32_t>(heavy_cap);
     for (int b = 0; b < 3; ++b) L.bucket[b] = c.keep_alloc<int32_t>(L.g.n);
-    k_buckets<<<grid_for(L.g.n, 256), 256, 0, c.s>>>(L.g.rp, L.g.n, L.heavy, L.bucket[0], L.bucket[1], L.bucket[2],
+    k_buckets<<<grid_for(L.g.n, 256), 256, 0, c.s>>>(L.g.rp, L.g.n, L.heavy_deg, heavy_cap, L.heavy, L.bucket[0], L.bucket[1], L.bucket[2],
                                                      d_cnt);
     GP_LAUNCHED(c);
     c.bytes += 8 * (L.g.n + 1) + 4 * L.g.n;
@@ -80,7 +84,7 @@ void build_heavy(Ctx& c, Level& L) {
     for (int b = 0; b < 3; ++b) L.nbucket[b] = c.h_pinned[b];
     L.nheavy = c.h_pinned[3];
     c.tmp->restore(mk);
-    // items: heavy row h covers [rp[v], rp[v+1]) in pieces of at most kHeavyDeg
+    // items: heavy row h covers [rp[v], rp[v+1]) in pieces of at most item_len
     std::vector<int64_t> rb((size_t)std::max<int64_t>(L.nheavy, 1)), re((size_t)std::max<int64_t>(L.nheavy, 1));
     if (L.nheavy > 0) {
         // row bounds of the heavy rows
@@ -98,10 +102,10 @@ void build_heavy(Ctx& c, Level& L) {
     for (int64_t h = 0; h < L.nheavy; ++h) {
         rows_first[h] = (int32_t)irow.size();
         int32_t cnt = 0;
-        for (int64_t b = rb[h]; b < re[h]; b += kItemLen) {
+        for (int64_t b = rb[h]; b < re[h]; b += L.item_len) {
             irow.push_back((int32_t)h);
             ib.push_back(b);
-            ie.push_back(std::min<int64_t>(b + kItemLen, re[h]));
+            ie.push_back(std::min<int64_t>(b + L.item_len, re[h]));
             ++cnt;
         }
         rows_items[h] = cnt;
@@ -194,7 +198,7 @@ __device__ __forceinline__ int32_t key_word(const MatchArgs& A, int64_t e) {
 
 template <int MODE>
 __device__ __forceinline__ bool match_ok(const MatchArgs& A, int64_t v, int32_t u, int64_t vwv) {
-    if (u == (int32_t)v) return false;
+    if (u == (int32_t)v || !GP_IN(u, A.g.n)) return false;
     if (MODE == 0) {
         if (A.any_matched && A.match[u] != -1) return false;
         if (A.check_vw && vwv + (A.g.vw ? A.g.vw[u] : 1) > A.maxvw) return false;
@@ -215,7 +219,8 @@ __device__ __forceinline__ void match_emit(const MatchArgs& A, bool valid, int64
     unsigned long long base = 0;
     if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)A.nkeys, (unsigned long long)__popc(m));
     base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (take) A.keys[base + __popc(m & ((1u << lane) - 1u))] = ((uint64_t)(uint32_t)best << A.nbits) | (uint64_t)v;
+    const int64_t idx = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (take && GP_IN(idx, A.g.n)) A.keys[idx] = ((uint64_t)(uint32_t)best << A.nbits) | (uint64_t)v;
 }
 
 template <int MODE, int TILE>
@@ -258,11 +263,19 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
         if (A.match[v] != -1 || (A.hdead && A.hdead[h])) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
         const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
         uint64_t bk = 0; int32_t bid = -1;
-        const int64_t end = A.item_end[blockIdx.x];
-        for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < end; e += blockDim.x) {
-            const int32_t u = __ldcs(&A.g.ci[e]);
-            if (match_ok<MODE>(A, v, u, vwv))
-                argmax_merge(bk, bid, edge_key(key_word(A, e), edge_hash(A.salt, (int32_t)v, u)), u);
+        const int64_t beg = A.item_beg[blockIdx.x], end = A.item_end[blockIdx.x];
+        const int32_t* kw = A.prio ? A.prio : A.g.ew;
+        const bool v4 = aligned16(A.g.ci) && aligned16(kw);
+        for (int64_t base = beg & ~(int64_t)3; base < end; base += 4 * (int64_t)blockDim.x) {
+            int32_t uu[4], ww[4];
+            const int64_t e4 = base + 4 * threadIdx.x;
+            ld4_row(A.g.ci, e4, beg, end, v4, -1, uu);
+            if (kw) ld4_row(kw, e4, beg, end, v4, 0, ww);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (uu[c] < 0 || !match_ok<MODE>(A, v, uu[c], vwv)) continue;
+                argmax_merge(bk, bid, edge_key(kw ? ww[c] : 1, edge_hash(A.salt, (int32_t)v, uu[c])), uu[c]);
+            }
         }
         block_argmax(bk, bid, sk, sid);
         const int nit = A.row_items[h];
@@ -304,18 +317,24 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
             if (valid) {
                 const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
                 const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
-                for (int64_t base = beg; base < end; base += 128) {
+                // 128 entries per sweep, four consecutive ones per lane (16-byte loads)
+                const int32_t* kw = A.prio ? A.prio : A.g.ew;
+                const bool v4 = aligned16(A.g.ci) && aligned16(kw);
+                for (int64_t base = beg & ~(int64_t)3; base < end; base += 128) {
                     int32_t uu[4], ww[4], mm[4], vv[4];
+                    const int64_t e4 = base + 4 * lane;
+                    ld4_row(A.g.ci, e4, beg, end, v4, -1, uu);
+                    if (kw) ld4_row(kw, e4, beg, end, v4, 0, ww);
+                    else {
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const int64_t e = base + c * 32 + lane;
-                        uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-                        ww[c] = e < end ? key_word(A, e) : 0;
+                        for (int c = 0; c < 4; ++c) ww[c] = 1;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        mm[c] = (MODE == 0 && A.any_matched && uu[c] >= 0) ? A.match[uu[c]] : -1;
-                        vv[c] = (MODE == 0 && A.check_vw && uu[c] >= 0 && A.g.vw) ? A.g.vw[uu[c]] : 1;
+                        const bool ok = uu[c] >= 0 && GP_IN(uu[c], A.g.n);
+                        if (!ok) uu[c] = -1;
+                        mm[c] = (MODE == 0 && A.any_matched && ok) ? A.match[uu[c]] : -1;
+                        vv[c] = (MODE == 0 && A.check_vw && ok && A.g.vw) ? A.g.vw[uu[c]] : 1;
                     }
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
@@ -340,8 +359,10 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
 // the worklists; a heavy one is flagged in hdead instead (heavy vertices are
 // not listed: their CTAs check match[] and hdead[] directly).  next_n[3]
 // counts the heavy vertices still live.
-__global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, const int32_t* l1, const int32_t* l2,
-                            int64_t n0, int64_t n1, int64_t n2, const int32_t* __restrict__ heavy, int64_t nheavy,
+__global__ void k_handshake(const int64_t* __restrict__ rp, int64_t n, int32_t heavy_deg, const int32_t* l0,
+                            const int32_t* l1,
+                            const int32_t* l2, int64_t n0, int64_t n1, int64_t n2, const int32_t* __restrict__ heavy,
+                            int64_t nheavy,
                             const int32_t* __restrict__ prop, int32_t* __restrict__ match, int64_t* __restrict__ pairs,
                             int32_t* nl0, int32_t* nl1, int32_t* nl2, int64_t* next_n, uint8_t* __restrict__ hdead) {
     int64_t local = 0;
@@ -359,7 +380,7 @@ __global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, c
         int64_t d = 0;
         if (v >= 0 && match[v] == -1 && !(is_heavy && hdead[i - n0 - n1 - n2])) {
             const int32_t u = prop[v];
-            if (u >= 0 && prop[u] == (int32_t)v) {
+            if (u >= 0 && GP_IN(u, n) && prop[u] == (int32_t)v) {
                 match[v] = u;
                 if (v < u) ++local;
             } else if (u < 0) {
@@ -371,16 +392,17 @@ __global__ void k_handshake(const int64_t* __restrict__ rp, const int32_t* l0, c
                 d = rp[v + 1] - rp[v];
             }
         }
-        warp_append(left && d <= kTile8, (int32_t)v, nl0, &next_n[0]);
-        warp_append(left && d > kTile8 && d <= kTile32, (int32_t)v, nl1, &next_n[1]);
-        warp_append(left && d > kTile32 && d <= kHeavyDeg, (int32_t)v, nl2, &next_n[2]);
+        warp_append(left && d <= kTile8, (int32_t)v, nl0, &next_n[0], n);
+        warp_append(left && d > kTile8 && d <= kTile32, (int32_t)v, nl1, &next_n[1], n);
+        warp_append(left && d > kTile32 && d <= heavy_deg, (int32_t)v, nl2, &next_n[2], n);
     }
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
     if ((threadIdx.x & 31) == 0 && local) atomicAdd((unsigned long long*)pairs, (unsigned long long)local);
 }
 
 // sorted (anchor << nbits | v) keys: pair ranks (0,1), (2,3), ... of each anchor group
-__global__ void k_twohop_pair(const uint64_t* __restrict__ keys, int64_t cnt, int nbits, const int32_t* __restrict__ vw,
+__global__ void k_twohop_pair(const uint64_t* __restrict__ keys, int64_t cnt, int64_t n, int nbits,
+                              const int32_t* __restrict__ vw,
                               int64_t maxvw, int32_t* __restrict__ match, int64_t* __restrict__ pairs) {
     int64_t local = 0;
     const uint64_t lowmask = (1ull << nbits) - 1;
@@ -394,6 +416,7 @@ __global__ void k_twohop_pair(const uint64_t* __restrict__ keys, int64_t cnt, in
         }
         if (((i - lo) & 1) || i + 1 >= cnt || (keys[i + 1] >> nbits) != a) continue;
         const int32_t x = (int32_t)(keys[i] & lowmask), y = (int32_t)(keys[i + 1] & lowmask);
+        if (!GP_IN(x, n) || !GP_IN(y, n)) continue;
         const int64_t wx = vw ? vw[x] : 1, wy = vw ? vw[y] : 1;
         if (wx + wy <= maxvw) { match[x] = y; match[y] = x; ++local; }
     }
@@ -464,7 +487,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         GP_LAUNCHED(c);
         int32_t** nxt = wl[r & 1];
         const int64_t tot = A.nlist[0] + A.nlist[1] + A.nlist[2] + L.nheavy;
-        k_handshake<<<grid_for(tot, 256), 256, 0, c.s>>>(g.rp, A.list[0], A.list[1], A.list[2], A.nlist[0], A.nlist[1],
+        k_handshake<<<grid_for(tot, 256), 256, 0, c.s>>>(g.rp, g.n, L.heavy_deg, A.list[0], A.list[1], A.list[2], A.nlist[0], A.nlist[1],
                                                          A.nlist[2], L.heavy, L.nheavy, prop, match, d_cnt, nxt[0],
                                                          nxt[1], nxt[2], d_cnt + 1, hdead);
         GP_LAUNCHED(c);
@@ -500,7 +523,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         if (cnt > 1) {
             GP_CUDA(cudaMemsetAsync(vals, 0, sizeof(int32_t) * cnt, c.s));
             radix_sort_pairs(c, keys, vals, keys2, vals2, cnt, 2 * nb);
-            k_twohop_pair<<<grid_for(cnt, 256), 256, 0, c.s>>>(keys, cnt, nb, g.vw, P.maxvw, match, d_cnt);
+            k_twohop_pair<<<grid_for(cnt, 256), 256, 0, c.s>>>(keys, cnt, g.n, nb, g.vw, P.maxvw, match, d_cnt);
             GP_LAUNCHED(c);
             c.bytes += 24 * cnt;
             pairs += read_i64(c, d_cnt);
@@ -527,6 +550,7 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
         const int32_t u = match[v];
         const bool rep = (u < 0 || v < u);
         const int64_t r = rep ? v : u;
+        if (!GP_IN(r, g.n)) continue;
         const int32_t cc = (int32_t)cid[r];
         cmap[v] = cc;
         if (rep) {
@@ -547,9 +571,11 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // the rank of its first position, with the weights of all its positions
 // summed; c itself is dropped.
 //
-// k_fill_mapped first streams every fine row, mapped through cmap, into the
-// walk layout (row c at off[c]); the dedup kernels then read that buffer
-// coalesced.  Tiers by row length d:
+// Tiers A, B, C and C2 read the walk straight from the fine CSR, mapping each
+// column id through cmap as they go, and read it once.  Tier D reads its rows
+// three times, so k_fill_walk_d first writes those rows, mapped, into a walk
+// layout (row c at off[c]).  Every tier writes its unique entries at off[c]
+// (a bound on the row) and k_contract_copy packs them.  Tiers by row length d:
 //   A  d <= 128        one warp, 256-slot table in shared memory
 //   B  d <= 1024       one warp, 2048-slot table in shared memory
 //   C  d <= 4096       one CTA of 256 threads, two-phase (first position kept by
@@ -559,7 +585,8 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 //   D  longer          pieces of 64K entries, one CTA each, table in global memory
 // A and B insert 32 entries at a time in walk order (match_any leaders), so
 // new neighbours get consecutive ranks; C and D rank first positions with one
-// block scan over per-thread contiguous segments.
+// block scan over per-thread contiguous segments.  The on-chip tables are
+// cleared once per CTA and afterwards only in the slots a row used.
 constexpr int TA_ROW = 128, TA_SLOTS = 256;
 constexpr int TB_ROW = 1024, TB_SLOTS = 2048, TB_WARPS = 4;
 constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 256;
@@ -571,53 +598,51 @@ __device__ __forceinline__ uint32_t slot_hash(int32_t key, int lg) {
     return ((uint32_t)key * 0x9E3779B1u) >> (32 - lg);
 }
 
-// warp per fine row (CTA per heavy fine row): mapped ids and weights in walk order
-__global__ void __launch_bounds__(256) k_fill_mapped(DGraph g, const int32_t* __restrict__ heavy,
-                                                     const int32_t* __restrict__ item_row,
-                                                     const int64_t* __restrict__ item_beg,
-                                                     const int64_t* __restrict__ item_end, int64_t nitems,
-                                                     const int32_t* __restrict__ cmap, const int32_t* __restrict__ mem,
-                                                     const int64_t* __restrict__ off, int32_t* __restrict__ mapped,
-                                                     int32_t* __restrict__ mw) {
-    auto fill_range = [&](int64_t x, int64_t from, int64_t to, int start, int stride) {
-        const int32_t cc = cmap[x];
-        const int32_t a = mem[2 * (int64_t)cc];
-        const int64_t base = off[cc] + ((int32_t)x == a ? 0 : g.rp[a + 1] - g.rp[a]);
-        const int64_t beg = g.rp[x];
-        for (int64_t e = from + start; e < to; e += stride) {
-            mapped[base + (e - beg)] = cmap[__ldcs(&g.ci[e])];
-            mw[base + (e - beg)] = g.ew ? __ldcs(&g.ew[e]) : 1;
-        }
-    };
-    if ((int64_t)blockIdx.x < nitems) {
-        fill_range(heavy[item_row[blockIdx.x]], item_beg[blockIdx.x], item_end[blockIdx.x], threadIdx.x, blockDim.x);
-        return;
-    }
-    const int lane = threadIdx.x & 31;
-    const int64_t wid = ((int64_t)(blockIdx.x - nitems) * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)(gridDim.x - nitems) * blockDim.x) >> 5;
-    for (int64_t x = wid; x < g.n; x += nw) {
-        if (g.rp[x + 1] - g.rp[x] > kHeavyDeg) continue;
-        fill_range(x, g.rp[x], g.rp[x + 1], lane, 32);
-    }
+// The walk of coarse row c in the fine CSR: positions [0, da) are a's row,
+// [da, deg) b's row (a = representative, b = partner or none).
+struct Walk {
+    int64_t ea, da, eb;
+    __device__ __forceinline__ int64_t entry(int64_t j) const { return j < da ? ea + j : eb + (j - da); }
+};
+__device__ __forceinline__ Walk walk_of(const DGraph& g, const int32_t* __restrict__ mem, int64_t c) {
+    const int32_t a = mem[2 * c], b = mem[2 * c + 1];
+    Walk W;
+    W.ea = g.rp[a];
+    W.da = g.rp[a + 1] - W.ea;
+    W.eb = b >= 0 ? g.rp[b] : 0;
+    return W;
+}
+// mapped id and weight of walk position j
+__device__ __forceinline__ void walk_load(const DGraph& g, const int32_t* __restrict__ cmap, const Walk& W, int64_t j,
+                                          int32_t& cu, int32_t& w) {
+    const int64_t e = W.entry(j);
+    const int32_t u = __ldcs(&g.ci[e]);
+    cu = GP_IN(u, g.n) ? cmap[u] : 0;
+    w = g.ew ? __ldcs(&g.ew[e]) : 1;
 }
 
+// tier-D rows in walk layout, by the pieces the tier-D kernels use
+struct TierD;
+__global__ void k_fill_walk_d(TierD D, DGraph g, const int32_t* __restrict__ cmap, const int32_t* __restrict__ mem,
+                              const int64_t* __restrict__ off, int32_t* __restrict__ mapped, int32_t* __restrict__ mw);
+
 // Ordered insertion of one walk by one warp into a shared-memory table.
-// okey/wacc: output ids and weights by rank (shared); returns the row length.
+// okey/wacc: output ids and weights by rank (shared), oslot: the slot of each
+// rank (the row's used slots, cleared afterwards); returns the row length.
 template <int SLOTS, class IdxT>
-__device__ __forceinline__ int32_t warp_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
-                                              int64_t o, int64_t deg, int32_t self, int32_t* key, IdxT* tidx,
+__device__ __forceinline__ int32_t warp_dedup(const DGraph& g, const int32_t* __restrict__ cmap, const Walk& W,
+                                              int64_t deg, int32_t self, int32_t* key, IdxT* tidx, IdxT* oslot,
                                               int32_t* okey, int32_t* wacc, int lg) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     int32_t count = 0;
     int32_t cu_next = -1, w_next = 0;
-    if (lane < deg) { cu_next = mapped[o + lane]; w_next = mw[o + lane]; }
+    if (lane < deg) walk_load(g, cmap, W, lane, cu_next, w_next);
     for (int64_t base = 0; base < deg; base += 32) {
         const int64_t j = base + lane;
         const int32_t cu = cu_next, wt = w_next;
         // prefetch the next chunk
-        if (j + 32 < deg) { cu_next = mapped[o + j + 32]; w_next = mw[o + j + 32]; }
+        if (j + 32 < deg) walk_load(g, cmap, W, j + 32, cu_next, w_next);
         const bool act = (j < deg) && cu != self;
         const uint32_t peers = __match_any_sync(0xffffffffu, act ? (uint32_t)cu : (0x80000000u | (uint32_t)lane));
         const int leader = __ffs(peers) - 1;
@@ -637,6 +662,7 @@ __device__ __forceinline__ int32_t warp_dedup(const int32_t* __restrict__ mapped
         if (isnew) {
             idx = count + __popc(newmask & lt);
             tidx[h] = (IdxT)idx;
+            oslot[idx] = (IdxT)h;
             okey[idx] = cu;
         }
         __syncwarp();
@@ -651,17 +677,17 @@ __device__ __forceinline__ int32_t warp_dedup(const int32_t* __restrict__ mapped
 
 template <int MAXROW, int SLOTS, class IdxT>
 __host__ __device__ constexpr size_t warp_dedup_smem() {
-    return ((sizeof(int32_t) * (SLOTS + 2 * MAXROW) + sizeof(IdxT) * SLOTS) + 15) & ~(size_t)15;
+    return ((sizeof(int32_t) * (SLOTS + 2 * MAXROW) + sizeof(IdxT) * (SLOTS + MAXROW)) + 15) & ~(size_t)15;
 }
 
 // tiers A (MAXROW 128) and B (MAXROW 1024): one warp per row
 template <int MAXROW, int SLOTS, int WARPS, class IdxT>
-__global__ void __launch_bounds__(WARPS * 32) k_dedup_warp(int64_t nc, int64_t minrow, const int64_t* __restrict__ off,
-                                                           const int64_t* __restrict__ cdeg,
-                                                           const int32_t* __restrict__ mapped,
-                                                           const int32_t* __restrict__ mw, int32_t* __restrict__ tci,
+__global__ void __launch_bounds__(WARPS * 32) k_dedup_warp(DGraph g, const int32_t* __restrict__ cmap,
+                                                           const int32_t* __restrict__ mem, int64_t nc, int64_t minrow,
+                                                           const int64_t* __restrict__ off,
+                                                           const int64_t* __restrict__ cdeg, int32_t* __restrict__ tci,
                                                            int32_t* __restrict__ tew, int32_t* __restrict__ cnt) {
-    // dynamic shared memory per warp: key[SLOTS] okey[MAXROW] wacc[MAXROW] idx[SLOTS]
+    // dynamic shared memory per warp: key[SLOTS] okey[MAXROW] wacc[MAXROW] idx[SLOTS] oslot[MAXROW]
     extern __shared__ int32_t dsm[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const size_t per_warp = warp_dedup_smem<MAXROW, SLOTS, IdxT>() / sizeof(int32_t);
@@ -669,6 +695,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_dedup_warp(int64_t nc, int64_t m
     int32_t* okey = key + SLOTS;
     int32_t* wacc = okey + MAXROW;
     IdxT* tidx = (IdxT*)(wacc + MAXROW);
+    IdxT* oslot = tidx + SLOTS;
     for (int i = lane; i < SLOTS; i += 32) key[i] = EMPTY_KEY;
     for (int i = lane; i < MAXROW; i += 32) wacc[i] = 0;
     __syncwarp();
@@ -680,13 +707,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_dedup_warp(int64_t nc, int64_t m
         const int64_t deg = cdeg[c];
         if (deg > MAXROW || deg < minrow) continue;
         const int64_t o = off[c];
-        const int32_t count = warp_dedup<SLOTS, IdxT>(mapped, mw, o, deg, (int32_t)c, key, tidx, okey, wacc, lg);
+        const int32_t count = warp_dedup<SLOTS, IdxT>(g, cmap, walk_of(g, mem, c), deg, (int32_t)c, key, tidx, oslot,
+                                                      okey, wacc, lg);
         for (int i = lane; i < count; i += 32) {
             tci[o + i] = okey[i];
             tew[o + i] = wacc[i];
             wacc[i] = 0;
+            key[oslot[i]] = EMPTY_KEY;
         }
-        for (int i = lane; i < SLOTS; i += 32) key[i] = EMPTY_KEY;
         if (lane == 0) cnt[c] = count;
         __syncwarp();
     }
@@ -735,23 +763,25 @@ __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_
     }
 }
 
-// tier C: one CTA per row, table in shared memory, two phases.  Phase 1
-// inserts every entry into a 64-bit slot (key + 1) << 32 | (deg - j), zero
-// meaning empty: the claiming compare-and-swap stores the first position
-// seen, later copies raise it by atomicMax (the largest deg - j is the first
-// occurrence); weights add up in wsum.  Phase 2: warps ballot the
-// first-occurrence flags of 32 consecutive positions into one word each, one
-// block scan over the word popcounts gives each word's base rank, and a
-// second strided sweep writes the first occurrences at base + rank within
-// the word.  words: 2 * ceil(deg/32) ints of scratch (bits, then prefix).
+// tiers C and C2: one CTA per row, table in shared memory, two phases.
+// Phase 1 reads the walk once (straight from the fine CSR) and inserts every
+// entry into a 64-bit slot (key + 1) << 32 | (deg - j), zero meaning empty:
+// the claiming compare-and-swap stores the first position seen, later copies
+// raise it by atomicMax (the largest deg - j is the first occurrence);
+// weights add up in wsum, and position j keeps its slot in hj[j].  Phase 2:
+// warps ballot the first-occurrence flags (slot value == deg - j) of 32
+// consecutive positions into one word each, one block scan over the word
+// popcounts gives each word's base rank, and a second sweep writes the first
+// occurrences at base + rank within the word, then empties their slots (each
+// used slot has exactly one first occurrence), so the table is clear for the
+// CTA's next row.  words: 2 * ceil(deg/32) ints (bits, then prefix).
+constexpr uint16_t NO_SLOT = 0xFFFF;
 template <int T>
-__device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw, int64_t o, int64_t deg,
-                          int32_t self, unsigned long long* slot, int32_t* wsum, int64_t S, int lg,
+__device__ void cta_dedup(const DGraph& g, const int32_t* __restrict__ cmap, const Walk& W, int64_t o, int64_t deg,
+                          int32_t self, unsigned long long* slot, int32_t* wsum, uint16_t* hj, int lg,
                           int32_t* words, int32_t* __restrict__ tci, int32_t* __restrict__ tew, int32_t* cnt_out,
                           int32_t* sh, int32_t* err) {
-    const uint32_t mask = (uint32_t)(S - 1);
-    for (int64_t i = threadIdx.x; i < S; i += T) { slot[i] = 0ull; wsum[i] = 0; }
-    __syncthreads();
+    const uint32_t S = 1u << lg, mask = S - 1u;
     for (int64_t base = 0; base < deg; base += 4 * T) {
         int32_t cu[4], wt[4];
         unsigned long long val[4], old[4];
@@ -759,8 +789,8 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int64_t j = base + c * T + threadIdx.x;
-            cu[c] = j < deg ? mapped[o + j] : self;
-            wt[c] = j < deg ? mw[o + j] : 0;
+            cu[c] = self; wt[c] = 0;
+            if (j < deg) walk_load(g, cmap, W, j, cu[c], wt[c]);
             val[c] = ((unsigned long long)((uint32_t)cu[c] + 1u) << 32) | (uint32_t)(deg - j);
         }
 #pragma unroll
@@ -770,17 +800,20 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            if (cu[c] == self) continue;
+            const int64_t j = base + c * T + threadIdx.x;
+            if (j >= deg) continue;
+            if (cu[c] == self) { hj[j] = NO_SLOT; continue; }
             const uint32_t tag = (uint32_t)cu[c] + 1u;
-            int64_t probe = 1;
+            uint32_t probe = 1;
             while (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag && probe < S) {
                 h[c] = (h[c] + 1) & mask;
                 old[c] = atomicCAS(&slot[h[c]], 0ull, val[c]);
                 ++probe;
             }
-            if (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag) { atomicExch(err, 1); continue; }
+            if (old[c] != 0ull && (uint32_t)(old[c] >> 32) != tag) { atomicExch(err, 1); hj[j] = NO_SLOT; continue; }
             if (old[c] != 0ull && old[c] < val[c]) atomicMax(&slot[h[c]], val[c]);
             atomicAdd(&wsum[h[c]], wt[c]);
+            hj[j] = (uint16_t)h[c];
         }
     }
     __syncthreads();
@@ -788,18 +821,12 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
     const int64_t nwords = (deg + 31) / 32;
     int32_t* bits = words;
     int32_t* wpre = words + nwords;
-    auto lookup = [&](int32_t cu) -> uint32_t {
-        const uint32_t tag = (uint32_t)cu + 1u;
-        uint32_t hh = slot_hash(cu, lg);
-        for (int64_t probe = 0; probe < S && (uint32_t)(slot[hh] >> 32) != tag; ++probe) hh = (hh + 1) & mask;
-        return hh;
-    };
     for (int64_t wi = wid; wi < nwords; wi += nwarp) {
         const int64_t j = wi * 32 + lane;
         bool first = false;
         if (j < deg) {
-            const int32_t cu = mapped[o + j];
-            if (cu != self) first = (uint32_t)slot[lookup(cu)] == (uint32_t)(deg - j);
+            const uint16_t hh = hj[j];
+            first = hh != NO_SLOT && (uint32_t)slot[hh] == (uint32_t)(deg - j);
         }
         const uint32_t word = __ballot_sync(0xffffffffu, first);
         if (lane == 0) bits[wi] = (int32_t)word;
@@ -818,42 +845,57 @@ __device__ void cta_dedup(const int32_t* __restrict__ mapped, const int32_t* __r
     for (int64_t wi = wid; wi < nwords; wi += nwarp) {
         const uint32_t word = (uint32_t)bits[wi];
         if (!((word >> lane) & 1u)) continue;
-        const int64_t j = wi * 32 + lane;
-        const int32_t cu = mapped[o + j];
+        const uint16_t hh = hj[wi * 32 + lane];
         const int32_t r = wpre[wi] + __popc(word & lt);
-        tci[o + r] = cu;
-        tew[o + r] = wsum[lookup(cu)];
+        if (!GP_IN(r, deg) || !GP_IN(hh, S)) continue;
+        tci[o + r] = (int32_t)((uint32_t)(slot[hh] >> 32) - 1u);
+        tew[o + r] = wsum[hh];
+    }
+    __syncthreads();
+    for (int64_t wi = wid; wi < nwords; wi += nwarp) {
+        const uint32_t word = (uint32_t)bits[wi];
+        if (!((word >> lane) & 1u)) continue;
+        const uint16_t hh = hj[wi * 32 + lane];
+        slot[hh] = 0ull;
+        wsum[hh] = 0;
     }
     if (threadIdx.x == 0) *cnt_out = tot;
     __syncthreads();
 }
 
 // shared memory of an on-chip tier: SLOTS 64-bit slots and int32 weight sums,
-// two words per 32 entries of the longest row
+// a slot id per walk position, two words per 32 entries of the longest row
 template <int SLOTS, int MAXROW>
 constexpr size_t cta_dedup_smem() {
-    return (sizeof(unsigned long long) + sizeof(int32_t)) * SLOTS + sizeof(int32_t) * 2 * ((MAXROW + 31) / 32);
+    return (sizeof(unsigned long long) + sizeof(int32_t)) * SLOTS + sizeof(uint16_t) * MAXROW +
+           sizeof(int32_t) * 2 * ((MAXROW + 31) / 32);
 }
 
 // tiers C and C2: table of at least twice the row length, at most SLOTS
 template <int T, int SLOTS, int MAXROW>
-__global__ void __launch_bounds__(T) k_dedup_cta_smem(const int32_t* __restrict__ list, int64_t nlist,
-                                                      const int64_t* __restrict__ off, const int64_t* __restrict__ cdeg,
-                                                      const int32_t* __restrict__ mapped, const int32_t* __restrict__ mw,
-                                                      int32_t* __restrict__ tci, int32_t* __restrict__ tew,
-                                                      int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+__global__ void __launch_bounds__(T) k_dedup_cta_smem(DGraph g, const int32_t* __restrict__ cmap,
+                                                      const int32_t* __restrict__ mem, const int32_t* __restrict__ list,
+                                                      int64_t nlist, const int64_t* __restrict__ off,
+                                                      const int64_t* __restrict__ cdeg, int32_t* __restrict__ tci,
+                                                      int32_t* __restrict__ tew, int32_t* __restrict__ cnt,
+                                                      int32_t* __restrict__ err) {
+    static_assert(SLOTS <= 65535, "slot ids are 16-bit");
     extern __shared__ __align__(16) unsigned char stab_raw[];
     unsigned long long* slot = (unsigned long long*)stab_raw;          // SLOTS
     int32_t* wsum = (int32_t*)(slot + SLOTS);                          // SLOTS
-    int32_t* words = wsum + SLOTS;                                     // 2 * MAXROW / 32
+    uint16_t* hj = (uint16_t*)(wsum + SLOTS);                          // MAXROW
+    int32_t* words = (int32_t*)(hj + ((MAXROW + 1) & ~1));             // 2 * MAXROW / 32
     __shared__ int32_t sh[33];
+    for (int i = threadIdx.x; i < SLOTS; i += T) { slot[i] = 0ull; wsum[i] = 0; }
+    __syncthreads();
     for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int64_t c = list[li];
         const int64_t deg = cdeg[c];
         int64_t S = 1;
         int lg = 0;
         while (S < 2 * deg && S < SLOTS) { S <<= 1; ++lg; }
-        cta_dedup<T>(mapped, mw, off[c], deg, (int32_t)c, slot, wsum, S, lg, words, tci, tew, &cnt[c], sh, err);
+        cta_dedup<T>(g, cmap, walk_of(g, mem, c), off[c], deg, (int32_t)c, slot, wsum, hj, lg, words, tci, tew,
+                     &cnt[c], sh, err);
     }
 }
 
@@ -882,6 +924,17 @@ struct TierD {
     int32_t* wcnt;          // their popcounts
     const int64_t* wpre;    // exclusive prefix of wcnt (+ total)
 };
+
+// mapped ids and weights of the tier-D rows in walk layout, one CTA per piece
+__global__ void __launch_bounds__(TD_T) k_fill_walk_d(TierD D, DGraph g, const int32_t* __restrict__ cmap,
+                                                      const int32_t* __restrict__ mem, const int64_t* __restrict__ off,
+                                                      int32_t* __restrict__ mapped, int32_t* __restrict__ mw) {
+    const int32_t c = D.rc[D.prow[blockIdx.x]];
+    const Walk W = walk_of(g, mem, c);
+    const int64_t o = off[c];
+    for (int64_t j = D.pbeg[blockIdx.x] + threadIdx.x; j < D.pend[blockIdx.x]; j += TD_T)
+        walk_load(g, cmap, W, j, mapped[o + j], mw[o + j]);
+}
 
 __device__ __forceinline__ uint32_t td_lookup(const unsigned long long* slot, int32_t cu, int lg) {
     const uint32_t mask = (1u << lg) - 1u;
@@ -980,6 +1033,7 @@ __global__ void __launch_bounds__(TD_T) k_td_write(TierD D, const int64_t* __res
         if (!((word >> lane) & 1u)) continue;
         const int32_t cu = mapped[o + wi * 32 + lane];
         const int64_t rank = D.wpre[rw + wi] - D.wpre[rw] + __popc(word & lt);
+        if (!GP_IN(rank, deg)) continue;
         tci[o + rank] = cu;
         tew[o + rank] = wsum[td_lookup(slot, cu, lg)];
     }
@@ -1038,20 +1092,15 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     memset_async(c, lcount, 0, 4 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
-        const int grid = (int)fine.nitems + grid_for(g.n * 32, 256, c.sm_count * c.ctas_per_sm);
-        k_fill_mapped<<<grid, 256, 0, c.s>>>(g, fine.heavy, fine.item_row, fine.item_beg, fine.item_end, fine.nitems,
-                                             fine.cmap, mem, off, mapped, mw);
-        GP_LAUNCHED(c);
-    }
-    {
         constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
         constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
         auto kA = k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>;
         auto kB = k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>;
-        kA<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, smA, c.s>>>(nc, 0, off, cdeg, mapped, mw, tci, tew, rowcnt);
+        kA<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, smA, c.s>>>(g, fine.cmap, mem, nc, 0, off, cdeg,
+                                                                                  tci, tew, rowcnt);
         GP_LAUNCHED(c);
-        kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * c.ctas_per_sm), TB_WARPS * 32, smB, c.s>>>(nc, TA_ROW + 1, off, cdeg,
-                                                                                        mapped, mw, tci, tew, rowcnt);
+        kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * c.ctas_per_sm), TB_WARPS * 32, smB, c.s>>>(
+            g, fine.cmap, mem, nc, TA_ROW + 1, off, cdeg, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
     k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listD, lcount);
@@ -1063,13 +1112,15 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         // one CTA per row: the block scheduler balances rows of unequal length
         k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>
             <<<(unsigned)std::min<int64_t>(nC, (int64_t)c.sm_count * c.ctas_per_sm), TC_T,
-               cta_dedup_smem<TC_SLOTS, TC_ROW>(), c.s>>>(listC, nC, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
+               cta_dedup_smem<TC_SLOTS, TC_ROW>(), c.s>>>(g, fine.cmap, mem, listC, nC, off, cdeg, tci, tew, rowcnt,
+                                                          err);
         GP_LAUNCHED(c);
     }
     if (nC2 > 0) {
         k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>
             <<<(unsigned)std::min<int64_t>(nC2, (int64_t)c.sm_count * c.ctas_per_sm), TC2_T,
-               cta_dedup_smem<TC2_SLOTS, TC2_ROW>(), c.s>>>(listC2, nC2, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
+               cta_dedup_smem<TC2_SLOTS, TC2_ROW>(), c.s>>>(g, fine.cmap, mem, listC2, nC2, off, cdeg, tci, tew, rowcnt,
+                                                            err);
         GP_LAUNCHED(c);
     }
     if (nD > 0) {
@@ -1125,6 +1176,8 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
         D.wpre = wpre;
         GP_CUDA(cudaMemsetAsync(D.slot, 0, sizeof(unsigned long long) * tab, c.s));
         GP_CUDA(cudaMemsetAsync(D.wsum, 0, sizeof(int32_t) * tab, c.s));
+        k_fill_walk_d<<<(unsigned)np, TD_T, 0, c.s>>>(D, g, fine.cmap, mem, off, mapped, mw);
+        GP_LAUNCHED(c);
         k_td_insert<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped, mw, err);
         GP_LAUNCHED(c);
         k_td_flags<<<(unsigned)np, TD_T, 0, c.s>>>(D, off, cdeg, mapped);

@@ -36,6 +36,49 @@ struct GpError : std::runtime_error {
         (ctx).launches++;                                                          \
     } while (0)
 
+// ---------------------------------------------------------------- bounds-checked build
+// Compiled with -DGP_CHECKED (libgp_b200_checked.so), GP_IN(i, n) tests a
+// data-dependent index before the access it guards: a failing check counts a
+// violation, records the first failing site (translation unit and line) and
+// the access is skipped.  In the regular build GP_IN is the constant true.
+// Each translation unit has its own counters; gp_checked_violations() sums
+// them.  This is the device-side stand-in for a memory checker: the checks
+// run at full speed on the GPU inside the normal kernels.
+#ifndef GP_TU_ID
+#define GP_TU_ID 0
+#endif
+#ifdef GP_CHECKED
+static __device__ unsigned long long g_chk_count;
+static __device__ unsigned long long g_chk_first;   // site + 1 of the first violation (0: none)
+__device__ __forceinline__ bool chk_in(int64_t i, int64_t n, int site) {
+    if (i >= 0 && i < n) return true;
+    atomicAdd(&g_chk_count, 1ull);
+    atomicCAS(&g_chk_first, 0ull, (unsigned long long)site + 1ull);
+    return false;
+}
+#define GP_IN(i, n) (::gp::chk_in((int64_t)(i), (int64_t)(n), GP_TU_ID * 100000 + __LINE__))
+typedef void (*chk_fetch_fn)(unsigned long long* count, unsigned long long* first, bool clear);
+void chk_register(chk_fetch_fn f);
+namespace {
+void chk_fetch_tu(unsigned long long* count, unsigned long long* first, bool clear) {
+    unsigned long long c = 0, f = 0;
+    cudaMemcpyFromSymbol(&c, g_chk_count, sizeof c);
+    cudaMemcpyFromSymbol(&f, g_chk_first, sizeof f);
+    if (clear) {
+        const unsigned long long z = 0;
+        cudaMemcpyToSymbol(g_chk_count, &z, sizeof z);
+        cudaMemcpyToSymbol(g_chk_first, &z, sizeof z);
+    }
+    *count += c;
+    if (!*first) *first = f;
+}
+struct ChkRegister { ChkRegister() { chk_register(&chk_fetch_tu); } };
+ChkRegister chk_register_tu;
+}  // namespace
+#else
+#define GP_IN(i, n) true
+#endif
+
 // ---------------------------------------------------------------- rules
 // The deterministic rule set shared with the CPU oracle (oracle/oracle.cpp
 // restates the same functions independently).
@@ -99,6 +142,25 @@ __device__ __forceinline__ void group_argmax64(uint32_t mask, uint64_t& k, int32
     id = (int32_t)mi;
 }
 #endif
+// Four consecutive entries [e, e + 4) of a row [beg, end) of a CSR array
+// (column ids, weights or per-entry priorities), e a multiple of 4: one
+// 16-byte streaming load when the array is 16-byte aligned (v4) and all four
+// lie inside the row, else element loads; positions outside the row read as
+// `fill`.  Nothing outside the row is read.
+__device__ __forceinline__ void ld4_row(const int32_t* __restrict__ a, int64_t e, int64_t beg, int64_t end, bool v4,
+                                        int32_t fill, int32_t (&x)[4]) {
+    if (v4 && e >= beg && e + 3 < end) {
+        const int4 t = __ldcs(reinterpret_cast<const int4*>(a + e));
+        x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x[c] = (e + c >= beg && e + c < end) ? __ldcs(a + e + c) : fill;
+    }
+}
+__host__ __device__ __forceinline__ bool aligned16(const void* p) {
+    return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
 template <class T>
 __device__ __forceinline__ T warp_incl_scan(T x) {
     const int lane = threadIdx.x & 31;
@@ -198,8 +260,8 @@ inline int grid_for(int64_t items, int per_block, int cap = 148 * 16) {
     if (g > cap) g = cap;
     return (int)g;
 }
-constexpr int kHeavyDeg = 2048;   // rows longer than this take whole CTAs
-constexpr int kItemLen = 16384;   // entries of one CTA item of a long row
+constexpr int kHeavyDeg = 2048;   // default: rows longer than this take whole CTAs (gp_options.heavy_deg)
+constexpr int kItemLen = 16384;   // default: entries of one CTA item of a long row (gp_options.item_len)
 
 // ---------------------------------------------------------------- primitives (gp_prims.cu)
 // exclusive scan; out may alias in; returns total on the host if total_out != nullptr

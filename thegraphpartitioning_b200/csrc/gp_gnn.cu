@@ -15,12 +15,27 @@
 //   h2_v = ReLU(W2 [h1_v; c_v] + b2)                                       (64)
 //   z_v  = Z h2_v                                                          (4)
 //   t_vu = sum_j A_j z_v[j] z_u[j] + beta log2(1+w)/8 + gamma (w/wdeg_v + w/wdeg_u) + delta
+//          + eta log2(1 + cn_vu)/7
+// cn_vu counts common neighbours through 128-bit neighbour signatures: bit
+// b(x) = fmix32(x * 0x9E3779B1) >> 25 is set in sig_v for every neighbour x
+// of v, and cn_vu = popcount(sig_v & sig_u) without the bits b(v) and b(u)
+// (an exact integer on both sides; at most 128).
 // t is symmetric bit-for-bit (the same products in the same order), so both
 // endpoints of an edge see the same priority clamp(round(t * 2^16) + 2^30).
 // Weights are stored in BF16 and every product is accumulated in FP32.
 // Training (binary cross-entropy on "edge ends up inside a part" labels) uses
 // the backward kernels below; no gradient needs a scatter because the graph
 // is symmetric (each row owner gathers what its neighbours would send).
+//
+// Move-order head: label-propagation candidates (vertex v proposing part
+// dest_v with integer gain g_v) are scored by a second small network,
+//   f_v = [sign(g) log2(1+|g|)/16, log2(1+deg_v)/8, log2(1+vw_v)/16, level/16]
+//   s_v = w2 . ReLU(W1 f_v + b1) + b2                (hidden 16)
+//   mprio_v = clamp(rint(s_v * 2^12), -2^30, 2^30)
+// and the afterburner treats the neighbours of higher (mprio, lower id) as
+// moved first, in place of the (gain, id) order.  It is trained on which
+// candidates of the plain partitioner end the level in their proposed part.
+#define GP_TU_ID 8   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 #include <cuda_bf16.h>
@@ -32,7 +47,11 @@ namespace gp {
 constexpr int H = 64, F0 = 4, MSG = 8, ZD = 4;
 constexpr int O_W1 = 0, O_B1 = O_W1 + H * 2 * F0, O_P = O_B1 + H, O_W2 = O_P + MSG * H, O_B2 = O_W2 + H * (H + MSG),
               O_Z = O_B2 + H, O_A = O_Z + ZD * H, O_BETA = O_A + ZD, O_GAMMA = O_BETA + 1, O_DELTA = O_GAMMA + 1,
-              NPARAM = O_DELTA + 1;
+              O_ETA = O_DELTA + 1, NPARAM = O_ETA + 1;
+constexpr int NEDGE = ZD + 4;   // A, beta, gamma, delta, eta
+// move-order head: W1[MH, MF] b1[MH] w2[MH] b2
+constexpr int MH = 16, MF = 4;
+constexpr int MO_W1 = 0, MO_B1 = MO_W1 + MH * MF, MO_W2 = MO_B1 + MH, MO_B2 = MO_W2 + MH, MNPARAM = MO_B2 + 1;
 
 }  // namespace gp
 
@@ -43,9 +62,17 @@ struct gp_gnn {
     float* adam_m = nullptr;
     float* adam_v = nullptr;
     int64_t step = 0;
-    float hedge[gp::ZD + 3] = {};     // host copy of the BF16-rounded A, beta, gamma, delta
+    float hedge[gp::NEDGE] = {};      // host copy of the BF16-rounded A, beta, gamma, delta, eta
     int32_t prio_bits = 16;           // priority = rint(logit * 2^prio_bits) + 2^30
     int32_t max_level = -1;           // learned priorities at levels <= max_level (-1: every level)
+    // move-order head (no allocation until its parameters are set)
+    float* mh_master = nullptr;
+    __nv_bfloat16* mh_w16 = nullptr;
+    float* mh_grad = nullptr;
+    float* mh_m = nullptr;
+    float* mh_v = nullptr;
+    int64_t mh_step = 0;
+    int32_t move_head = 0;            // 1: the learned V-cycle orders moves by the head
     gp::Arena arena;                  // per-vertex activations
     gp::Arena keep;                   // row buckets of graphs scored outside a V-cycle
 };
@@ -338,9 +365,43 @@ __global__ void __launch_bounds__(128) k_gnn_l2(int64_t n, const __nv_bfloat16* 
     }
 }
 
+// signature bit of vertex x (0..127)
+__host__ __device__ __forceinline__ uint32_t nb_bit(int32_t x) { return fmix32((uint32_t)x * 0x9E3779B1u) >> 25; }
+
+// 128-bit neighbour signature of every vertex, one warp per row
+__global__ void k_gnn_sig(DGraph g, uint4* __restrict__ sig) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t v = wid; v < g.n; v += nw) {
+        uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+        for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32) {
+            const uint32_t b = nb_bit(__ldcs(&g.ci[e])), m = 1u << (b & 31), q = b >> 5;
+            w0 |= q == 0 ? m : 0u; w1 |= q == 1 ? m : 0u; w2 |= q == 2 ? m : 0u; w3 |= q == 3 ? m : 0u;
+        }
+        w0 = __reduce_or_sync(0xffffffffu, w0); w1 = __reduce_or_sync(0xffffffffu, w1);
+        w2 = __reduce_or_sync(0xffffffffu, w2); w3 = __reduce_or_sync(0xffffffffu, w3);
+        if (lane == 0) sig[v] = make_uint4(w0, w1, w2, w3);
+    }
+}
+
+// log2(1 + common-neighbour count) / 7 of the entry (v, u)
+__device__ __forceinline__ float cn_feat(const uint4* __restrict__ sig, int64_t v, int64_t u) {
+    const uint4 a = sig[v], b = sig[u];
+    uint32_t m0 = a.x & b.x, m1 = a.y & b.y, m2 = a.z & b.z, m3 = a.w & b.w;
+    const uint32_t bv = nb_bit((int32_t)v), bu = nb_bit((int32_t)u);
+    const uint32_t cv = ~(1u << (bv & 31)), cu = ~(1u << (bu & 31));
+    m0 &= (bv >> 5) == 0 ? cv : ~0u; m1 &= (bv >> 5) == 1 ? cv : ~0u;
+    m2 &= (bv >> 5) == 2 ? cv : ~0u; m3 &= (bv >> 5) == 3 ? cv : ~0u;
+    m0 &= (bu >> 5) == 0 ? cu : ~0u; m1 &= (bu >> 5) == 1 ? cu : ~0u;
+    m2 &= (bu >> 5) == 2 ? cu : ~0u; m3 &= (bu >> 5) == 3 ? cu : ~0u;
+    const int cnt = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+    return log2f(1.f + (float)cnt) * (1.f / 7.f);
+}
+
 __device__ __forceinline__ float edge_logit(const float* __restrict__ sA, float beta, float gamma, float delta,
-                                            const float* zv, const float* __restrict__ z, int64_t u, float w,
-                                            float wdv, float wdu) {
+                                            float eta, float fcn, const float* zv, const float* __restrict__ z,
+                                            int64_t u, float w, float wdv, float wdu) {
     const float4 q = reinterpret_cast<const float4*>(z)[u];
     const float zu[ZD] = {q.x, q.y, q.z, q.w};
     float t = 0.f;
@@ -348,7 +409,8 @@ __device__ __forceinline__ float edge_logit(const float* __restrict__ sA, float 
     for (int j = 0; j < ZD; ++j) t += sA[j] * (zv[j] * zu[j]);
     t += beta * (log2f(1.f + w) * 0.125f);
     t += gamma * (w / wdv + w / wdu);
-    return t + delta;
+    t += delta;
+    return t + eta * fcn;
 }
 
 // clamp(rint(t * 2^bits) + 2^30, 0, 2^31 - 128) with pscale = 2^bits; the
@@ -363,16 +425,16 @@ __device__ __forceinline__ int32_t logit_prio(float t, float pscale) {
 // per entry: priority (matching) and/or logit (checks)
 struct EdgeOp {
     DGraph g;
-    const float* z; const float* wdeg;
-    float A[ZD]; float beta, gamma, delta, pscale;
+    const float* z; const float* wdeg; const uint4* sig;
+    float A[ZD]; float beta, gamma, delta, eta, pscale;
     int32_t* prio; float* logit;
     __device__ void operator()(int64_t v, int64_t e) const {
         const int64_t u = __ldcs(&g.ci[e]);
         float zv[ZD];
         const float4 q = reinterpret_cast<const float4*>(z)[v];
         zv[0] = q.x; zv[1] = q.y; zv[2] = q.z; zv[3] = q.w;
-        const float t = edge_logit(A, beta, gamma, delta, zv, z, u, g.ew ? (float)__ldcs(&g.ew[e]) : 1.f, wdeg[v],
-                                   wdeg[u]);
+        const float t = edge_logit(A, beta, gamma, delta, eta, cn_feat(sig, v, u), zv, z, u,
+                                   g.ew ? (float)__ldcs(&g.ew[e]) : 1.f, wdeg[v], wdeg[u]);
         if (prio) prio[e] = logit_prio(t, pscale);
         if (logit) logit[e] = t;
     }
@@ -381,19 +443,20 @@ struct EdgeOp {
 // ------------------------------------------------------------------ training
 // loss and dt per entry; dz_v = 2 sum_u dt_vu A (.) z_u; gradients of A, beta, gamma, delta
 __global__ void k_gnn_edge_bwd(DGraph g, const __nv_bfloat16* __restrict__ w, const float* __restrict__ z,
-                               const float* __restrict__ wdeg, const uint8_t* __restrict__ label, float inv_e,
-                               float* __restrict__ dz, float* __restrict__ grad, float* __restrict__ loss) {
+                               const float* __restrict__ wdeg, const uint4* __restrict__ sig,
+                               const uint8_t* __restrict__ label, float inv_e, float* __restrict__ dz,
+                               float* __restrict__ grad, float* __restrict__ loss) {
     __shared__ float sA[ZD];
-    __shared__ float sc[3];
-    __shared__ float sg[ZD + 4];
+    __shared__ float sc[4];
+    __shared__ float sg[ZD + 5];
     if (threadIdx.x < ZD) sA[threadIdx.x] = wload(w, O_A + threadIdx.x);
-    if (threadIdx.x < 3) sc[threadIdx.x] = wload(w, O_BETA + threadIdx.x);
-    if (threadIdx.x < ZD + 4) sg[threadIdx.x] = 0.f;
+    if (threadIdx.x < 4) sc[threadIdx.x] = wload(w, O_BETA + threadIdx.x);
+    if (threadIdx.x < ZD + 5) sg[threadIdx.x] = 0.f;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    float gA[ZD] = {0.f, 0.f, 0.f, 0.f}, gb = 0.f, gg = 0.f, gd = 0.f, ls = 0.f;
+    float gA[ZD] = {0.f, 0.f, 0.f, 0.f}, gb = 0.f, gg = 0.f, gd = 0.f, ge = 0.f, ls = 0.f;
     for (int64_t v = wid; v < g.n; v += nw) {
         float zv[ZD], dzv[ZD];
 #pragma unroll
@@ -402,7 +465,8 @@ __global__ void k_gnn_edge_bwd(DGraph g, const __nv_bfloat16* __restrict__ w, co
         for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32) {
             const int64_t u = g.ci[e];
             const float we = g.ew ? (float)g.ew[e] : 1.f;
-            const float t = edge_logit(sA, sc[0], sc[1], sc[2], zv, z, u, we, wdv, wdeg[u]);
+            const float fcn = cn_feat(sig, v, u);
+            const float t = edge_logit(sA, sc[0], sc[1], sc[2], sc[3], fcn, zv, z, u, we, wdv, wdeg[u]);
             const float y = label[e] ? 1.f : 0.f;
             const float s = 1.f / (1.f + expf(-t));
             // BCE with logits, stable form
@@ -417,6 +481,7 @@ __global__ void k_gnn_edge_bwd(DGraph g, const __nv_bfloat16* __restrict__ w, co
             gb += dt * (log2f(1.f + we) * 0.125f);
             gg += dt * (we / wdv + we / wdeg[u]);
             gd += dt;
+            ge += dt * fcn;
         }
         warp_reduce_vec<ZD>(dzv);
         if (lane < ZD) {
@@ -426,16 +491,17 @@ __global__ void k_gnn_edge_bwd(DGraph g, const __nv_bfloat16* __restrict__ w, co
             dz[ZD * v + lane] = r;
         }
     }
-    float part[ZD + 4] = {gA[0], gA[1], gA[2], gA[3], gb, gg, gd, ls};
-    warp_reduce_vec<ZD + 4>(part);
+    float part[ZD + 5] = {gA[0], gA[1], gA[2], gA[3], gb, gg, gd, ls, ge};
+    warp_reduce_vec<ZD + 5>(part);
     if (lane == 0)
-        for (int j = 0; j < ZD + 4; ++j) atomicAdd(&sg[j], part[j]);
+        for (int j = 0; j < ZD + 5; ++j) atomicAdd(&sg[j], part[j]);
     __syncthreads();
     if (threadIdx.x < ZD) atomicAdd(&grad[O_A + threadIdx.x], sg[threadIdx.x]);
     if (threadIdx.x == ZD) atomicAdd(&grad[O_BETA], sg[ZD]);
     if (threadIdx.x == ZD + 1) atomicAdd(&grad[O_GAMMA], sg[ZD + 1]);
     if (threadIdx.x == ZD + 2) atomicAdd(&grad[O_DELTA], sg[ZD + 2]);
     if (threadIdx.x == ZD + 3) atomicAdd(loss, sg[ZD + 3]);
+    if (threadIdx.x == ZD + 4) atomicAdd(&grad[O_ETA], sg[ZD + 4]);
 }
 
 // dpre2 = (Z^T dz) * [h2 > 0]; dh1 (direct part) and dc from W2^T dpre2; thread per vertex
@@ -592,6 +658,7 @@ __global__ void k_gnn_to_bf16(int np, const float* __restrict__ master, __nv_bfl
 // ------------------------------------------------------------------ host
 struct GnnActs {
     float *x, *wdeg, *a, *m, *c, *z, *h1, *h2;
+    uint4* sig;               // neighbour signatures (common-neighbour feature)
 };
 
 static void gnn_forward(Ctx& c, const gp_gnn* G, const Level& L, int level, bool keep, GnnActs& A) {
@@ -618,6 +685,9 @@ static void gnn_forward(Ctx& c, const gp_gnn* G, const Level& L, int level, bool
     }
     k_gnn_vfeat<<<vg, 256, 0, c.s>>>(n, g.rp, g.vw, (float)level, g.ew ? 0 : 1, (float4*)A.x, A.wdeg);
     GP_LAUNCHED(c);
+    A.sig = (uint4*)c.tmp->alloc(sizeof(uint4) * (size_t)std::max<int64_t>(n, 1));
+    k_gnn_sig<<<grid_for(n * 32, 256, c.sm_count * 16), 256, 0, c.s>>>(g, A.sig);
+    GP_LAUNCHED(c);
     k_gnn_rowsum<F0><<<rg, 256, 0, c.s>>>(R, ValRow4{g.ci, (const float4*)A.x}, FinMean<F0>{g.rp, A.a}, ipart);
     GP_LAUNCHED(c);
     if (L.nheavy) { k_gnn_rowsum_heavy<F0><<<hg, 128, 0, c.s>>>(R, FinMean<F0>{g.rp, A.a}, ipart); GP_LAUNCHED(c); }
@@ -637,7 +707,8 @@ static EdgeOp edge_op(const gp_gnn* G, const DGraph& g, const GnnActs& A, int32_
     EdgeOp op;
     op.g = g; op.z = A.z; op.wdeg = A.wdeg;
     for (int j = 0; j < ZD; ++j) op.A[j] = G->hedge[j];
-    op.beta = G->hedge[ZD]; op.gamma = G->hedge[ZD + 1]; op.delta = G->hedge[ZD + 2];
+    op.beta = G->hedge[ZD]; op.gamma = G->hedge[ZD + 1]; op.delta = G->hedge[ZD + 2]; op.eta = G->hedge[ZD + 3];
+    op.sig = A.sig;
     op.pscale = ldexpf(1.f, G->prio_bits);
     op.prio = prio; op.logit = logit;
     return op;
@@ -653,6 +724,139 @@ static void gnn_edges(Ctx& c, const gp_gnn* G, const Level& L, const GnnActs& A,
 
 bool gnn_scores_level(const gp_gnn* G, int level) { return G->max_level < 0 || level <= G->max_level; }
 
+// ------------------------------------------------------------------ move-order head
+__device__ __forceinline__ void move_features(int32_t gain, int64_t deg, int32_t vw, int level, float (&f)[MF]) {
+    const float mag = log2f(1.f + fabsf((float)gain)) * (1.f / 16.f);
+    f[0] = gain < 0 ? -mag : mag;
+    f[1] = log2f(1.f + (float)deg) * 0.125f;
+    f[2] = log2f(1.f + (float)vw) * (1.f / 16.f);
+    f[3] = (float)level * (1.f / 16.f);
+}
+
+// score of one feature row from parameters staged in shared memory (FP32 accumulate)
+__device__ __forceinline__ float move_score(const float* __restrict__ sp, const float (&f)[MF], float (&h)[MH]) {
+    float s = sp[MO_B2];
+#pragma unroll
+    for (int i = 0; i < MH; ++i) {
+        float a = sp[MO_B1 + i];
+#pragma unroll
+        for (int j = 0; j < MF; ++j) a += sp[MO_W1 + i * MF + j] * f[j];
+        h[i] = a;
+        s += sp[MO_W2 + i] * (a > 0.f ? a : 0.f);
+    }
+    return s;
+}
+
+__device__ __forceinline__ int32_t move_prio(float s) {
+    const float q = fminf(fmaxf(rintf(s * 4096.f), -1073741824.f), 1073741824.f);
+    return (int32_t)q;
+}
+
+__device__ __forceinline__ void stage_head(const __nv_bfloat16* __restrict__ w, float* sp) {
+    for (int i = threadIdx.x; i < MNPARAM; i += blockDim.x) sp[i] = wload(w, i);
+    __syncthreads();
+}
+
+// features of every candidate (dest >= 0; others get zeros)
+__global__ void k_move_feat(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ vw,
+                            const int32_t* __restrict__ dest, const int32_t* __restrict__ gain, int level,
+                            float* __restrict__ feat) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        float f[MF] = {0.f, 0.f, 0.f, 0.f};
+        if (dest[v] >= 0) move_features(gain[v], rp[v + 1] - rp[v], vw ? vw[v] : 1, level, f);
+#pragma unroll
+        for (int j = 0; j < MF; ++j) feat[MF * v + j] = f[j];
+    }
+}
+
+// move priorities of the candidates of one label-propagation step
+__global__ void k_move_prio(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ vw,
+                            const int32_t* __restrict__ dest, const int32_t* __restrict__ gain, int level,
+                            const __nv_bfloat16* __restrict__ w, int32_t* __restrict__ mp) {
+    __shared__ float sp[MNPARAM];
+    stage_head(w, sp);
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int32_t r = 0;
+        if (dest[v] >= 0) {
+            float f[MF], h[MH];
+            move_features(gain[v], rp[v + 1] - rp[v], vw ? vw[v] : 1, level, f);
+            r = move_prio(move_score(sp, f, h));
+        }
+        mp[v] = r;
+    }
+}
+
+// scores (and priorities) of feature rows
+__global__ void k_move_score(int64_t ns, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
+                             float* __restrict__ score, int32_t* __restrict__ prio) {
+    __shared__ float sp[MNPARAM];
+    stage_head(w, sp);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (int64_t)gridDim.x * blockDim.x) {
+        float f[MF], h[MH];
+#pragma unroll
+        for (int j = 0; j < MF; ++j) f[j] = feat[MF * i + j];
+        const float s = move_score(sp, f, h);
+        if (score) score[i] = s;
+        if (prio) prio[i] = move_prio(s);
+    }
+}
+
+// mean binary cross-entropy of the scores against the labels and its
+// gradient: per-thread register accumulation over a strided run of
+// samples, then warp and block reductions (no atomic per sample)
+__global__ void __launch_bounds__(256) k_move_grad(int64_t ns, const float* __restrict__ feat,
+                                                   const uint8_t* __restrict__ label,
+                                                   const __nv_bfloat16* __restrict__ w, float inv_n,
+                                                   float* __restrict__ grad, float* __restrict__ loss) {
+    __shared__ float sp[MNPARAM];
+    __shared__ float sg[MNPARAM + 1];
+    for (int i = threadIdx.x; i <= MNPARAM; i += blockDim.x) sg[i] = 0.f;
+    stage_head(w, sp);
+    float g[MNPARAM + 1];
+#pragma unroll
+    for (int j = 0; j <= MNPARAM; ++j) g[j] = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (int64_t)gridDim.x * blockDim.x) {
+        float f[MF], h[MH];
+#pragma unroll
+        for (int j = 0; j < MF; ++j) f[j] = feat[MF * i + j];
+        const float s = move_score(sp, f, h);
+        const float y = label[i] ? 1.f : 0.f;
+        g[MNPARAM] += (fmaxf(s, 0.f) - s * y + log1pf(expf(-fabsf(s)))) * inv_n;
+        const float ds = (1.f / (1.f + expf(-s)) - y) * inv_n;
+        g[MO_B2] += ds;
+#pragma unroll
+        for (int k2 = 0; k2 < MH; ++k2) {
+            const float a = h[k2];
+            g[MO_W2 + k2] += ds * (a > 0.f ? a : 0.f);
+            const float dh = a > 0.f ? ds * sp[MO_W2 + k2] : 0.f;
+            g[MO_B1 + k2] += dh;
+#pragma unroll
+            for (int j = 0; j < MF; ++j) g[MO_W1 + k2 * MF + j] += dh * f[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j <= MNPARAM; ++j) {
+        float x = g[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&sg[j], x);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < MNPARAM; j += blockDim.x) atomicAdd(&grad[j], sg[j]);
+    if (threadIdx.x == 0) atomicAdd(loss, sg[MNPARAM]);
+}
+
+bool gnn_has_move_head(const gp_gnn* G) { return G && G->move_head; }
+
+// move priorities of one label-propagation step of the learned V-cycle
+void gnn_move_priorities(Ctx& c, const gp_gnn* G, const DGraph& g, int level, const int32_t* dest,
+                         const int32_t* gain, int32_t* mp) {
+    k_move_prio<<<grid_for(g.n, 256, c.sm_count * 8), 256, 0, c.s>>>(g.n, g.rp, g.vw, dest, gain, level, G->mh_w16,
+                                                                   mp);
+    GP_LAUNCHED(c);
+    c.bytes += 8 * (g.n + 1) + 16 * g.n;
+}
+
 // learned matching priorities of one level (called by the V-cycle driver)
 void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, int32_t* prio) {
     auto mk = c.tmp->save();
@@ -664,10 +868,10 @@ void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, in
 
 // BF16-rounded edge coefficients mirrored on the host (they travel as kernel arguments)
 static void refresh_host_edge(gp_gnn* G, cudaStream_t s) {
-    __nv_bfloat16 h[ZD + 3];
+    __nv_bfloat16 h[NEDGE];
     GP_CUDA(cudaMemcpyAsync(h, G->w16 + O_A, sizeof h, cudaMemcpyDeviceToHost, s));
     GP_CUDA(cudaStreamSynchronize(s));
-    for (int j = 0; j < ZD + 3; ++j) G->hedge[j] = __bfloat162float(h[j]);
+    for (int j = 0; j < NEDGE; ++j) G->hedge[j] = __bfloat162float(h[j]);
 }
 
 // loss and gradients of one graph (gradients accumulated into G->grad)
@@ -689,7 +893,7 @@ static float gnn_grad(Ctx& c, gp_gnn* G, const Level& L, int level, const uint8_
     memset_async(c, loss, 0, sizeof(float));
     const int wg = grid_for(n * 32, 256, c.sm_count * 8), tg = grid_for(n, 128, c.sm_count * 8);
     const float inv_e = g.m > 0 ? 1.f / (float)g.m : 0.f;
-    k_gnn_edge_bwd<<<wg, 256, 0, c.s>>>(g, G->w16, A.z, A.wdeg, label, inv_e, dz, G->grad, loss);
+    k_gnn_edge_bwd<<<wg, 256, 0, c.s>>>(g, G->w16, A.z, A.wdeg, A.sig, label, inv_e, dz, G->grad, loss);
     GP_LAUNCHED(c);
     k_gnn_l2_bwd<<<tg, 128, 0, c.s>>>(n, G->w16, dz, A.h2, dpre2, dh1, dc);
     GP_LAUNCHED(c);
@@ -797,6 +1001,7 @@ int gp_gnn_destroy(gp_gnn* G) {
     return gnn_guard([&] {
         if (!G) return;
         cudaFree(G->master); cudaFree(G->w16); cudaFree(G->grad); cudaFree(G->adam_m); cudaFree(G->adam_v);
+        cudaFree(G->mh_master); cudaFree(G->mh_w16); cudaFree(G->mh_grad); cudaFree(G->mh_m); cudaFree(G->mh_v);
         delete G;
     });
 }
@@ -907,6 +1112,108 @@ int gp_gnn_train_step_device(gp_gnn* G, int32_t ngraphs, const int64_t* ns, cons
         GP_LAUNCHED(call.c);
         refresh_host_edge(G, call.c.s);
         if (loss_out) *loss_out = tot / (float)ngraphs;
+    });
+}
+
+// ---- move-order head
+int gp_gnn_move_num_params(void) { return MNPARAM; }
+
+int gp_gnn_set_move_params(gp_gnn* G, const float* params, int32_t np) {
+    return gnn_guard([&] {
+        if (!G) throw GpError(GP_EINVAL, "null model");
+        if (np == 0) { G->move_head = 0; return; }
+        if (!params || np != MNPARAM) throw GpError(GP_EINVAL, "bad move-head parameter array");
+        if (!G->mh_master) {
+            GP_CUDA(cudaMalloc(&G->mh_master, sizeof(float) * MNPARAM));
+            GP_CUDA(cudaMalloc(&G->mh_w16, sizeof(__nv_bfloat16) * MNPARAM));
+            GP_CUDA(cudaMalloc(&G->mh_grad, sizeof(float) * (MNPARAM + 1)));   // + the loss
+            GP_CUDA(cudaMalloc(&G->mh_m, sizeof(float) * MNPARAM));
+            GP_CUDA(cudaMalloc(&G->mh_v, sizeof(float) * MNPARAM));
+        }
+        GP_CUDA(cudaMemcpy(G->mh_master, params, sizeof(float) * MNPARAM, cudaMemcpyHostToDevice));
+        k_gnn_to_bf16<<<1, 128>>>(MNPARAM, G->mh_master, G->mh_w16);
+        GP_CUDA(cudaGetLastError());
+        GP_CUDA(cudaMemset(G->mh_m, 0, sizeof(float) * MNPARAM));
+        GP_CUDA(cudaMemset(G->mh_v, 0, sizeof(float) * MNPARAM));
+        GP_CUDA(cudaDeviceSynchronize());
+        G->mh_step = 0;
+        G->move_head = 1;
+    });
+}
+
+int gp_gnn_get_move_params(const gp_gnn* G, float* params, int32_t np) {
+    return gnn_guard([&] {
+        if (!G || !params || np != MNPARAM) throw GpError(GP_EINVAL, "bad move-head parameter array");
+        if (!G->move_head) throw GpError(GP_EINVAL, "the model has no move-order head");
+        GP_CUDA(cudaMemcpy(params, G->mh_master, sizeof(float) * MNPARAM, cudaMemcpyDeviceToHost));
+    });
+}
+
+int gp_gnn_move_features_device(int64_t n, const int64_t* d_rowptr, const int32_t* d_vwgt, const int32_t* d_dest,
+                                const int32_t* d_gain, int32_t level, void* stream, float* d_feat_out) {
+    return gnn_guard([&] {
+        if (n < 0 || (n > 0 && (!d_rowptr || !d_dest || !d_gain || !d_feat_out))) throw GpError(GP_EINVAL, "bad arguments");
+        if (n == 0) return;
+        k_move_feat<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, d_rowptr, d_vwgt, d_dest, d_gain, level,
+                                                                       d_feat_out);
+        GP_CUDA(cudaGetLastError());
+        GP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    });
+}
+
+int gp_gnn_move_scores_device(gp_gnn* G, int64_t ns, const float* d_feat, void* stream, float* d_score_out,
+                              int32_t* d_prio_out) {
+    return gnn_guard([&] {
+        if (!G || !G->move_head) throw GpError(GP_EINVAL, "the model has no move-order head");
+        if (ns < 0 || (ns > 0 && !d_feat)) throw GpError(GP_EINVAL, "bad arguments");
+        if (ns == 0) return;
+        k_move_score<<<grid_for(ns, 256), 256, 0, (cudaStream_t)stream>>>(ns, d_feat, G->mh_w16, d_score_out,
+                                                                         d_prio_out);
+        GP_CUDA(cudaGetLastError());
+        GP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    });
+}
+
+static float move_grad(gp_gnn* G, int64_t ns, const float* d_feat, const uint8_t* d_label, cudaStream_t s) {
+    GP_CUDA(cudaMemsetAsync(G->mh_grad, 0, sizeof(float) * (MNPARAM + 1), s));
+    float* d_loss = G->mh_grad + MNPARAM;
+    if (ns > 0) {
+        k_move_grad<<<grid_for(ns, 256, 148 * 4), 256, 0, s>>>(ns, d_feat, d_label, G->mh_w16, 1.f / (float)ns,
+                                                               G->mh_grad, d_loss);
+        GP_CUDA(cudaGetLastError());
+    }
+    float h = 0.f;
+    GP_CUDA(cudaMemcpyAsync(&h, d_loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    GP_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+int gp_gnn_move_grad_device(gp_gnn* G, int64_t ns, const float* d_feat, const uint8_t* d_label, void* stream,
+                            float* loss_out, float* grad_out) {
+    return gnn_guard([&] {
+        if (!G || !G->move_head) throw GpError(GP_EINVAL, "the model has no move-order head");
+        if (ns < 0 || (ns > 0 && (!d_feat || !d_label))) throw GpError(GP_EINVAL, "bad arguments");
+        const float l = move_grad(G, ns, d_feat, d_label, (cudaStream_t)stream);
+        if (loss_out) *loss_out = l;
+        if (grad_out) GP_CUDA(cudaMemcpy(grad_out, G->mh_grad, sizeof(float) * MNPARAM, cudaMemcpyDeviceToHost));
+    });
+}
+
+int gp_gnn_move_train_step_device(gp_gnn* G, int64_t ns, const float* d_feat, const uint8_t* d_label, float lr,
+                                  void* stream, float* loss_out) {
+    return gnn_guard([&] {
+        if (!G || !G->move_head) throw GpError(GP_EINVAL, "the model has no move-order head");
+        if (ns <= 0 || !d_feat || !d_label) throw GpError(GP_EINVAL, "bad arguments");
+        cudaStream_t s = (cudaStream_t)stream;
+        const float l = move_grad(G, ns, d_feat, d_label, s);
+        G->mh_step += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)G->mh_step), c2 = 1.f - powf(b2, (float)G->mh_step);
+        k_gnn_adam<<<1, 128, 0, s>>>(MNPARAM, G->mh_master, G->mh_w16, G->mh_grad, G->mh_m, G->mh_v, lr, b1, b2,
+                                     1e-8f, c1, c2);
+        GP_CUDA(cudaGetLastError());
+        GP_CUDA(cudaStreamSynchronize(s));
+        if (loss_out) *loss_out = l;
     });
 }
 

@@ -17,6 +17,7 @@
 // ranges identified by their first part.  Trials run in parallel, one per CTA;
 // the kept trial is the balanced one with the lowest cut (lowest trial id on
 // ties), else the one with the smallest heaviest part.
+#define GP_TU_ID 3   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 namespace gp {

@@ -34,11 +34,13 @@ constexpr int kTile32 = 32;       // bucket 1: degree <= 32
 struct Level {
     DGraph g;
     int32_t* cmap = nullptr;      // fine -> coarse map to the next coarser level
-    int32_t* heavy = nullptr;     // vertices with degree > kHeavyDeg
+    int32_t heavy_deg = kHeavyDeg; // rows longer than this are heavy (whole CTAs)
+    int32_t item_len = kItemLen;  // entries of one CTA item of a heavy row
+    int32_t* heavy = nullptr;     // vertices with degree > heavy_deg
     int64_t nheavy = 0;
     int32_t* bucket[3] = {nullptr, nullptr, nullptr};
     int64_t nbucket[3] = {0, 0, 0};
-    // heavy rows split into items of at most kHeavyDeg entries, one CTA each
+    // heavy rows split into items of at most item_len entries, one CTA each
     int32_t* item_row = nullptr;   // index into heavy[]
     int64_t* item_beg = nullptr;   // entry range of the item
     int64_t* item_end = nullptr;
@@ -70,6 +72,10 @@ inline void resolve_options(const gp_options* in, int32_t k, gp_options* o) {
     if (d.strong_after <= 0) d.strong_after = 2;
     if (d.check_input == 0) d.check_input = 1;
     if (d.ctas_per_sm <= 0) d.ctas_per_sm = 64;
+    if (d.heavy_deg <= 0) d.heavy_deg = kHeavyDeg;
+    d.heavy_deg = std::min(std::max(d.heavy_deg, 64), 65536);
+    if (d.item_len <= 0) d.item_len = kItemLen;
+    d.item_len = std::min(std::max(d.item_len, d.heavy_deg), 1 << 20);
     *o = d;
 }
 
@@ -97,6 +103,7 @@ struct RefineBufs {
     int pcb = 1;                  // its bytes per vertex (1: k <= 256, 2: k <= 1024)
     int32_t* dest = nullptr;
     int32_t* gain = nullptr;
+    int32_t* mp = nullptr;        // learned move priorities of a label-propagation step
     uint8_t* lock = nullptr;
     uint8_t* lock_next = nullptr;
     int64_t* pw = nullptr;        // k
@@ -118,9 +125,54 @@ struct RefineBufs {
 enum StatusSlot { S_CROSS = 0, S_MAXPW = 1, S_MODE = 2, S_NL0 = 3, S_NL1 = 4, S_LIGHT = 5, S_NL2 = 6, S_CDEG = 7,
                   S_NRESET = 8, S_STEP_MOVES = 8, S_NSLOTS = 16 };
 
-// gp_api.cu
+// CUDA events of the phases of one V-cycle
+struct Timer {
+    cudaEvent_t e[8];
+    Timer() { for (auto& x : e) cudaEventCreate(&x); }
+    ~Timer() { for (auto& x : e) cudaEventDestroy(x); }
+    Timer(const Timer&) = delete;
+    Timer& operator=(const Timer&) = delete;
+    double ms(int a, int b) { float t = 0; cudaEventElapsedTime(&t, e[a], e[b]); return t; }
+};
+
+// State of one V-cycle between its phases (hierarchy and buffers live in the
+// keep arena of the context that ran vc_begin).  Counters of the contexts
+// that ran its phases are moved here by take().
+struct VState {
+    Params P;
+    DGraph g0;
+    std::vector<Level> lv;
+    RefineBufs B;
+    Timer tm;
+    int L = 0, best_trial = -1, iters = 0;
+    int refined_to = 1;          // finest level refined so far (L + 1: none)
+    int64_t launches = 0, bytes = 0, conn_launches = 0, conn_bytes = 0;
+    double ms_conn = 0, ms_gnn = 0;
+    void take(Ctx& c) {
+        launches += c.launches; bytes += c.bytes; ms_conn += c.ms_conn; ms_gnn += c.ms_gnn;
+        conn_launches += c.conn_launches; conn_bytes += c.conn_bytes;
+        c.launches = 0; c.bytes = 0; c.ms_conn = 0; c.ms_gnn = 0; c.conn_launches = 0; c.conn_bytes = 0;
+    }
+};
+
+// gp_api.cu: the V-cycle as three phases (run_vcycle runs them in a row)
+void vc_begin(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
+              VState& S, const Tracer& tr, const gp_gnn* gnn = nullptr);
+void vc_level(Ctx& c, VState& S, int l, const Tracer& tr);
+void vc_end(Ctx& c, VState& S, int32_t* d_out, gp_stats* st);
 void run_vcycle(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t seed, const gp_options* opt,
                 int32_t* d_out, gp_stats* st, const Tracer& tr, const gp_gnn* gnn = nullptr);
+
+// gp_refine.cu: one-block levels of many V-cycles in one persistent launch.
+// chain_add (thread-safe) queues the coarsest levels of S that one block
+// refines (scratch from c.keep) and returns their count; chain_run launches
+// the persistent kernel over every queued chain, then advances each
+// VState's refined_to past its chain.
+struct ChainBatch;
+ChainBatch* chain_batch_new();
+void chain_batch_delete(ChainBatch* cb);
+int chain_add(Ctx& c, ChainBatch* cb, VState& S);
+void chain_run(Ctx& c, ChainBatch* cb);
 int check_args(int64_t n, int32_t k, float imbalance);
 extern thread_local std::string t_err;
 
@@ -136,6 +188,9 @@ void initpart_smem_caps();
 // gp_gnn.cu
 void gnn_level_priorities(Ctx& c, const gp_gnn* G, const Level& L, int level, int32_t* prio);
 bool gnn_scores_level(const gp_gnn* G, int level);   // false: edge weights at this level
+bool gnn_has_move_head(const gp_gnn* G);
+void gnn_move_priorities(Ctx& c, const gp_gnn* G, const DGraph& g, int level, const int32_t* dest,
+                         const int32_t* gain, int32_t* mp);
 
 // gp_coarsen.cu
 void build_heavy(Ctx& c, Level& L);

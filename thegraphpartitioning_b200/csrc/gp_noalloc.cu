@@ -20,6 +20,7 @@
 //   (cudaGetSymbolAddress); make that first call before any stream capture;
 // * no cudaMalloc, cudaFree, cudaMallocHost or other allocating routine is
 //   called; results are copied into the caller's host memory.
+#define GP_TU_ID 6   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 #include <mutex>

@@ -6,6 +6,7 @@
 // scan of the digit-major (digit, tile) count table, and a scatter kernel that
 // ranks items stably inside the tile with warp match/ballot and per-warp digit
 // counters in shared memory.
+#define GP_TU_ID 1   // site ids of the bounds-checked build
 #include "gp_common.cuh"
 
 #include <algorithm>
@@ -260,8 +261,10 @@ __global__ void __launch_bounds__(RS_T) k_rs_scatter(const uint64_t* __restrict_
             __syncwarp();
             if (ok) {
                 int64_t pos = dbase[dg[i]] + basecnt + __popc(peers & lt);
-                kout[pos] = k[i];
-                vout[pos] = v[i];
+                if (GP_IN(pos, n)) {
+                    kout[pos] = k[i];
+                    vout[pos] = v[i];
+                }
                 if (lane == leader) wcnt[w][dg[i]] = basecnt + __popc(peers);
             }
             __syncwarp();

@@ -23,9 +23,11 @@
 //               exclusive prefix sums of vertex weight select the moves that
 //               cover each source's excess and fit each destination's capacity
 //               (weak) or the concatenated free capacities (strong).
+#define GP_TU_ID 4   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
 #include <cstring>
+#include <mutex>
 
 namespace gp {
 
@@ -108,8 +110,8 @@ struct ConnArgs {
 
 // part id of neighbour u from the gather copy (read-only in the kernel)
 template <class PT>
-__device__ __forceinline__ int32_t gpart(const void* pc, int32_t u) {
-    return (int32_t)__ldg((const PT*)pc + u);
+__device__ __forceinline__ int32_t gpart(const void* pc, int32_t u, int64_t n) {
+    return GP_IN(u, n) ? (int32_t)__ldg((const PT*)pc + u) : 0;
 }
 
 // rebalance moves keep the gather copy of part current (pcb bytes per id)
@@ -119,19 +121,20 @@ __device__ __forceinline__ void store_pc(void* pc, int pcb, int64_t v, int32_t d
     else ((uint16_t*)pc)[v] = (uint16_t)d;
 }
 
-__device__ __forceinline__ void hist_add(int32_t* hist, int32_t q, int32_t w, bool valid) {
-    if (valid) atomicAdd(&hist[q], w);
+__device__ __forceinline__ void hist_add(int32_t* hist, int32_t q, int32_t w, bool valid, int32_t k) {
+    if (valid && GP_IN(q, k)) atomicAdd(&hist[q], w);
 }
 
 // warp-aggregated append of the lanes with take set
-__device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, int64_t* count) {
+__device__ __forceinline__ void warp_push(bool take, int32_t v, int32_t* list, int64_t* count, int64_t cap) {
     const uint32_t m = __ballot_sync(0xffffffffu, take);
     if (!m) return;
     const int lane = threadIdx.x & 31;
     unsigned long long base = 0;
     if (lane == __ffs(m) - 1) base = atomicAdd((unsigned long long*)count, (unsigned long long)__popc(m));
     base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (take) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+    const int64_t idx = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (take && GP_IN(idx, cap)) list[idx] = v;
 }
 
 // decision of one row from its best other part (bq, bk), own connectivity
@@ -177,7 +180,7 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     const int64_t e = beg + tl;
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
-    if (has) { q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e])); w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
+    if (has) { q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]), A.g.n); w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
     const uint32_t tmask = TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (tix * TILE));
     const int32_t cross = (int32_t)__reduce_add_sync(tmask, (has && q != p) ? (uint32_t)w : 0u);
     const int32_t tot = (int32_t)__reduce_add_sync(tmask, (uint32_t)w);
@@ -194,7 +197,8 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
         take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
         if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
-    warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))]);
+    warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))],
+              A.g.n);
 }
 
 // bucket 2: one row per warp, shared-memory histogram.  The row is swept
@@ -213,21 +217,24 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
     const int32_t p = A.part[v];
     const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
     int32_t cross = 0, tot = 0;
-    for (int64_t base = beg; base < end; base += 128) {
+    // 128 entries per sweep, four consecutive ones per lane (16-byte loads)
+    const bool v4 = aligned16(A.g.ci) && aligned16(A.g.ew);
+    for (int64_t base = beg & ~(int64_t)3; base < end; base += 128) {
         int32_t u[4], w[4], q[4];
+        const int64_t e4 = base + 4 * lane;
+        ld4_row(A.g.ci, e4, beg, end, v4, -1, u);
+        if (A.g.ew) ld4_row(A.g.ew, e4, beg, end, v4, 0, w);
+        else {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int64_t e = base + c * 32 + lane;
-            u[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-            w[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
+            for (int c = 0; c < 4; ++c) w[c] = u[c] >= 0 ? 1 : 0;
         }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? gpart<PT>(A.pc, u[c]) : -1;
+        for (int c = 0; c < 4; ++c) q[c] = u[c] >= 0 ? gpart<PT>(A.pc, u[c], A.g.n) : -1;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             tot += w[c];
             if (q[c] >= 0 && q[c] != p) cross += w[c];
-            if (active) hist_add(hist, q[c], w[c], q[c] >= 0 && q[c] != p);
+            if (active) hist_add(hist, q[c], w[c], q[c] >= 0 && q[c] != p, A.k);
         }
     }
     cross = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)cross);
@@ -248,12 +255,16 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
             for (int q = lane; q < A.k; q += 32) hist[q] = 0;
         } else {
             for (int64_t e = beg + lane; e < end; e += 32) {
-                const int32_t q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]));
+                const int32_t q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]), A.g.n);
+                if (!GP_IN(q, A.k)) continue;
                 if (q != p && (mode != MODE_RB || !over[q])) argmax_u32(lh, lq, (uint32_t)hist[q], q);
             }
             group_argmax_u32(0xffffffffu, bk, bq, lh, lq);
             __syncwarp();
-            for (int64_t e = beg + lane; e < end; e += 32) hist[gpart<PT>(A.pc, __ldcs(&A.g.ci[e]))] = 0;
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const int32_t q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]), A.g.n);
+                if (GP_IN(q, A.k)) hist[q] = 0;
+            }
         }
         __syncwarp();
     }
@@ -263,11 +274,11 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
         take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
         if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
-    warp_push(take, (int32_t)v, A.clist[2], &A.status[S_NL2]);
+    warp_push(take, (int32_t)v, A.clist[2], &A.status[S_NL2], A.g.n);
 }
 
 template <class PT>
-__global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
+__global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
     extern __shared__ int32_t csm[];
     const int32_t k = A.k;
     const int64_t Lmax = A.Lmax;
@@ -321,21 +332,23 @@ __global__ void __launch_bounds__(RT) k_conn(ConnArgs A) {
         const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
         const int64_t beg = A.item_beg[blockIdx.x], end = A.item_end[blockIdx.x];
         int64_t cross = 0, tot = 0;
-        for (int64_t base = beg; base < end; base += 4 * RT) {
+        const bool v4 = aligned16(A.g.ci) && aligned16(A.g.ew);
+        for (int64_t base = beg & ~(int64_t)3; base < end; base += 4 * RT) {
             int32_t uu[4], ww[4], qq[4];
+            const int64_t e4 = base + 4 * threadIdx.x;
+            ld4_row(A.g.ci, e4, beg, end, v4, -1, uu);
+            if (A.g.ew) ld4_row(A.g.ew, e4, beg, end, v4, 0, ww);
+            else {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int64_t e = base + c * RT + threadIdx.x;
-                uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-                ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
+                for (int c = 0; c < 4; ++c) ww[c] = uu[c] >= 0 ? 1 : 0;
             }
 #pragma unroll
-            for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? gpart<PT>(A.pc, uu[c]) : -1;
+            for (int c = 0; c < 4; ++c) qq[c] = uu[c] >= 0 ? gpart<PT>(A.pc, uu[c], A.g.n) : -1;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 tot += ww[c];
                 if (qq[c] >= 0 && qq[c] != p) cross += ww[c];
-                if (active) hist_add(hist, qq[c], ww[c], qq[c] >= 0 && qq[c] != p);
+                if (active) hist_add(hist, qq[c], ww[c], qq[c] >= 0 && qq[c] != p, k);
             }
         }
         cross = warp_sum(cross); tot = warp_sum(tot);
@@ -438,7 +451,8 @@ __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v
                                            const void* pc, const int32_t* __restrict__ dest,
                                            const int32_t* __restrict__ gain) {
     const int32_t u = __ldcs(&g.ci[e]);
-    int32_t pu = gpart<PT>(pc, u);
+    if (!GP_IN(u, g.n)) return 0;
+    int32_t pu = gpart<PT>(pc, u, g.n);
     const int32_t du = dest[u];
     if (du >= 0) {
         const int32_t gu = gain[u];
@@ -475,6 +489,7 @@ struct ApplyArgs {
 template <class PT>
 __device__ __forceinline__ void ab_commit(const ApplyArgs& A, int64_t v, int32_t p, int32_t d, int64_t* delta,
                                           int64_t& moves) {
+    if (!GP_IN(d, A.k) || !GP_IN(p, A.k)) return;
     A.part_next[v] = d;
     if (A.pc_next) ((PT*)A.pc_next)[v] = (PT)d;
     A.lock_next[v] = 1;
@@ -507,22 +522,25 @@ __device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* 
     const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
     const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
     int32_t g2 = 0;
-    for (int64_t base = beg; base < end; base += 128) {
+    const bool v4 = aligned16(A.g.ci) && aligned16(A.g.ew);
+    for (int64_t base = beg & ~(int64_t)3; base < end; base += 128) {
         int32_t uu[4], ww[4], pu[4], du[4];
+        const int64_t e4 = base + 4 * lane;
+        ld4_row(A.g.ci, e4, beg, end, v4, -1, uu);
+        if (A.g.ew) ld4_row(A.g.ew, e4, beg, end, v4, 0, ww);
+        else {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int64_t e = base + c * 32 + lane;
-            uu[c] = e < end ? __ldcs(&A.g.ci[e]) : -1;
-            ww[c] = e < end ? (A.g.ew ? __ldcs(&A.g.ew[e]) : 1) : 0;
+            for (int c = 0; c < 4; ++c) ww[c] = uu[c] >= 0 ? 1 : 0;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            pu[c] = uu[c] >= 0 ? gpart<PT>(A.pc, uu[c]) : -1;
-            du[c] = uu[c] >= 0 ? A.dest[uu[c]] : -1;
+            const bool ok = uu[c] >= 0 && GP_IN(uu[c], A.g.n);
+            pu[c] = ok ? gpart<PT>(A.pc, uu[c], A.g.n) : -1;
+            du[c] = ok ? A.dest[uu[c]] : -1;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            if (uu[c] < 0) continue;
+            if (uu[c] < 0 || pu[c] < 0) continue;
             int32_t q = pu[c];
             if (du[c] >= 0) {
                 const int32_t gu = A.gain[uu[c]];
@@ -1045,8 +1063,9 @@ __global__ void __launch_bounds__(CT, 1) k_rb_step_cta(RbCta R, int mode, int64_
     if (threadIdx.x == 0) *moves_out += moves;
 }
 
-__global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
-    extern __shared__ __align__(16) unsigned char rsm[];
+// the whole refinement loop of one level by one block of CT threads; rsm:
+// cta_refine_smem(k) bytes of dynamic shared memory
+__device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
     const int32_t k = R.k;
     const int64_t Lmax = R.Lmax, n = R.g.n;
     int64_t* s_pw = (int64_t*)rsm;               // k: current part weights
@@ -1203,6 +1222,48 @@ __global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
     if (threadIdx.x == 0) R.out[0] = steps;
 }
 
+__global__ void __launch_bounds__(CT, 1) k_refine_cta(CtaRefineArgs R) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    cta_refine_level(R, rsm);
+}
+
+// ------------------------------------------------------------------ batched one-block levels
+// A chain is the run of one graph's levels, coarsest first, that one block
+// refines (at most kCtaMaxN vertices, no row longer than kHeavyDeg).  The
+// persistent kernel k_refine_chains takes chains from a device work queue (an
+// atomic ticket over the chains, ordered by cost, largest first) and, for
+// each level of the chain, projects the coarser level's partition and runs
+// the level's whole refinement loop, with no host round trip between
+// levels or iterations.  Chains are independent, so no block ever waits for
+// another.
+struct ChainItem {
+    CtaRefineArgs R;          // R.part receives the projected partition
+    const int32_t* cmap;      // fine -> coarse map of this level (nullptr: coarsest level, no projection)
+    const int32_t* pcoarse;   // refined partition of the next coarser level
+};
+
+__global__ void __launch_bounds__(CT, 1) k_refine_chains(const int32_t* __restrict__ chain_first,
+                                                         const int32_t* __restrict__ chain_len, int32_t nchains,
+                                                         const ChainItem* __restrict__ items, int32_t* ticket) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    __shared__ int32_t s_chain;
+    for (;;) {
+        if (threadIdx.x == 0) s_chain = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int32_t ch = s_chain;
+        __syncthreads();
+        if (ch >= nchains) return;
+        for (int32_t t = 0; t < chain_len[ch]; ++t) {
+            const ChainItem& it = items[chain_first[ch] + t];
+            if (it.cmap)
+                for (int64_t v = threadIdx.x; v < it.R.g.n; v += CT) it.R.part[v] = it.pcoarse[it.cmap[v]];
+            __syncthreads();
+            cta_refine_level(it.R, rsm);
+            __syncthreads();
+        }
+    }
+}
+
 static size_t cta_refine_smem(int32_t k) {
     const size_t head = (((size_t)(4 * k + 1) * 8 + k + 15) & ~(size_t)15);
     const size_t hist = sizeof(int32_t) * CW * (size_t)k, keys = sizeof(uint64_t) * kCtaMaxN;
@@ -1213,6 +1274,8 @@ void refine_smem_caps() {
     GP_CUDA(cudaFuncSetAttribute(k_refine_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_refine_smem(GP_MAX_K)));
     GP_CUDA(cudaFuncSetAttribute(k_rb_step_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_refine_smem(GP_MAX_K)));
+    GP_CUDA(cudaFuncSetAttribute(k_refine_chains, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_refine_smem(GP_MAX_K)));
 }
 
@@ -1263,6 +1326,108 @@ static int refine_level_cta(Ctx& c, const Level& L, const Params& P, RefineBufs&
     }
     c.tmp->restore(mk);
     return steps;
+}
+
+static bool chain_level_ok(const Level& L, const Params& P) {
+    return L.nheavy == 0 && L.g.n <= kCtaMaxN && P.k <= GP_MAX_K;
+}
+
+struct ChainBatch {
+    std::mutex mu;
+    std::vector<ChainItem> items;
+    struct Rec { VState* S; int32_t first, len; int64_t cost; };
+    std::vector<Rec> chains;
+    int32_t kmax = 2;
+};
+
+ChainBatch* chain_batch_new() { return new ChainBatch(); }
+void chain_batch_delete(ChainBatch* cb) { delete cb; }
+
+int chain_add(Ctx& c, ChainBatch* cb, VState& S) {
+    const Params& P = S.P;
+    if (P.k <= 1 || S.refined_to != S.L + 1) return 0;
+    int s = S.L + 1;
+    while (s > 0 && chain_level_ok(S.lv[s - 1], P)) --s;
+    const int len = S.L + 1 - s;
+    if (len == 0) return 0;
+    int64_t nmax = 1, cost = 0;
+    for (int l = s; l <= S.L; ++l) { nmax = std::max(nmax, S.lv[l].g.n); cost += S.lv[l].g.n + S.lv[l].g.m; }
+    RefineBufs& B = S.B;
+    int64_t* pre = c.keep_alloc<int64_t>(nmax);
+    int32_t* flag = c.keep_alloc<int32_t>(nmax);
+    uint64_t* gkeys = c.keep_alloc<uint64_t>(nmax);
+    std::vector<ChainItem> mine((size_t)len);
+    for (int t = 0; t < len; ++t) {
+        const int l = S.L - t;
+        const Level& L = S.lv[l];
+        ChainItem& it = mine[t];
+        CtaRefineArgs& R = it.R;
+        R.g = L.g; R.k = P.k; R.Lmax = P.Lmax; R.den = P.o.lp_filter_den; R.max_iters = P.o.refine_max_iters;
+        R.patience = P.o.refine_patience; R.strong_after = P.o.strong_after;
+        for (int b = 0; b < 3; ++b) { R.bucket[b] = L.bucket[b]; R.nbucket[b] = L.nbucket[b]; R.clist[b] = B.clist[b]; }
+        // the partition alternates between the two part buffers level by level
+        int32_t* cur = (t & 1) ? B.part_next : B.part;
+        int32_t* other = (t & 1) ? B.part : B.part_next;
+        R.part = cur; R.part_next = other; R.lock = B.lock; R.lock_next = B.lock_next; R.best = B.best;
+        R.pw = B.pw; R.dest = B.dest; R.gain = B.gain; R.status = B.status;
+        R.pre = pre; R.flag = flag; R.gkeys = gkeys;
+        R.tr_arrays = nullptr; R.tr_scalars = nullptr;
+        R.out = nullptr;   // set by chain_run
+        it.cmap = t == 0 ? nullptr : L.cmap;
+        it.pcoarse = other;
+    }
+    std::lock_guard<std::mutex> lk(cb->mu);
+    cb->chains.push_back({&S, (int32_t)cb->items.size(), (int32_t)len, cost});
+    cb->items.insert(cb->items.end(), mine.begin(), mine.end());
+    cb->kmax = std::max(cb->kmax, P.k);
+    return len;
+}
+
+void chain_run(Ctx& c, ChainBatch* cb) {
+    const int32_t nch = (int32_t)cb->chains.size();
+    if (nch == 0) return;
+    // largest chains first
+    std::vector<int32_t> order((size_t)nch);
+    for (int32_t i = 0; i < nch; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return cb->chains[a].cost > cb->chains[b].cost; });
+    std::vector<int32_t> hfirst((size_t)nch), hlen((size_t)nch);
+    for (int32_t i = 0; i < nch; ++i) { hfirst[i] = cb->chains[order[i]].first; hlen[i] = cb->chains[order[i]].len; }
+    auto mk = c.tmp->save();
+    const int64_t ni = (int64_t)cb->items.size();
+    ChainItem* d_items = (ChainItem*)c.tmp->alloc(sizeof(ChainItem) * (size_t)ni);
+    int32_t* d_first = c.tmp_alloc<int32_t>(nch);
+    int32_t* d_len = c.tmp_alloc<int32_t>(nch);
+    int32_t* d_ticket = c.tmp_alloc<int32_t>(1);
+    int64_t* d_steps = c.tmp_alloc<int64_t>(ni);
+    for (int64_t i = 0; i < ni; ++i) cb->items[i].R.out = d_steps + i;
+    GP_CUDA(cudaMemcpyAsync(d_items, cb->items.data(), sizeof(ChainItem) * (size_t)ni, cudaMemcpyHostToDevice, c.s));
+    GP_CUDA(cudaMemcpyAsync(d_first, hfirst.data(), sizeof(int32_t) * nch, cudaMemcpyHostToDevice, c.s));
+    GP_CUDA(cudaMemcpyAsync(d_len, hlen.data(), sizeof(int32_t) * nch, cudaMemcpyHostToDevice, c.s));
+    memset_async(c, d_ticket, 0, sizeof(int32_t));
+    const size_t smem = cta_refine_smem(cb->kmax);
+    int per_sm = 1;
+    GP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_chains, CT, smem));
+    const int grid = (int)std::min<int64_t>(nch, (int64_t)std::max(per_sm, 1) * c.sm_count);
+    k_refine_chains<<<grid, CT, smem, c.s>>>(d_first, d_len, nch, d_items, d_ticket);
+    GP_LAUNCHED(c);
+    // steps of every level; the partition ends in the buffer of the last level
+    std::vector<int64_t> steps((size_t)ni);
+    GP_CUDA(cudaMemcpyAsync(steps.data(), d_steps, sizeof(int64_t) * (size_t)ni, cudaMemcpyDeviceToHost, c.s));
+    c.sync();
+    c.tmp->restore(mk);
+    for (auto& rec : cb->chains) {
+        VState& S = *rec.S;
+        for (int t = 0; t < rec.len; ++t) {
+            const Level& L = S.lv[S.L - t];
+            const int64_t n = L.g.n;
+            const int64_t st = steps[rec.first + t];
+            S.iters += (int)st;
+            S.bytes += (st + 1) * (L.scan_bytes() + 13 * n) + st * (9 * n + 16 * n) + (t ? 12 * n : 0);
+        }
+        if ((rec.len - 1) & 1) std::swap(S.B.part, S.B.part_next);
+        S.refined_to = S.L + 1 - rec.len;
+    }
 }
 
 // ------------------------------------------------------------------ level controller
@@ -1395,6 +1560,21 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             AA.status = B.status; AA.part_next = B.part_next; AA.lock_next = B.lock_next; AA.pw = B.pw;
             AA.moves_out = moves_d;
             AA.pc = B.pc; AA.pc_next = B.pc_next;
+            if (B.mp && P.gnn && gnn_has_move_head(P.gnn)) {
+                // learned order of the afterburner: (move priority, id) instead of (gain, id)
+                gnn_move_priorities(c, P.gnn, g, level, B.dest, B.gain, B.mp);
+                AA.gain = B.mp;
+                if (tr.on()) {
+                    std::vector<int32_t> hm((size_t)n);
+                    GP_CUDA(cudaMemcpyAsync(hm.data(), B.mp, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.s));
+                    c.sync();
+                    gp_trace_event ev;
+                    memset(&ev, 0, sizeof ev);
+                    ev.kind = GP_TR_MOVE_PRIO; ev.level = level; ev.iter = it; ev.n = n; ev.m = g.m;
+                    ev.a0 = hm.data();
+                    tr.emit(ev);
+                }
+            }
             if (B.pcb == 1) k_lp_apply<uint8_t><<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
             else k_lp_apply<uint16_t><<<grid, RT, sizeof(int64_t) * k, c.s>>>(AA);
             GP_LAUNCHED(c);

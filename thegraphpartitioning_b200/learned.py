@@ -19,8 +19,16 @@ After training, the priority resolution (GNN.prio_bits) is chosen on a
 validation set of larger graphs from the same families (other seeds): the
 value with the lowest geometric-mean cut relative to the plain method.
 
+Move-order head: the label-propagation candidates of the plain partitioner
+(every LP step of every level, from the REFINE_ITER trace: proposed part and
+integer gain) are labelled 1 when the candidate ends its level in the part it
+proposed (LEVEL_DONE), i.e. the moves the plain method finally accepts.  The
+head is trained on these rows with its own device kernels and kept only when
+it lowers the geometric-mean cut on the validation set.
+
     python -m thegraphpartitioning_b200.learned train --graphs 2000 --out gnn_weights.npz
-    python -m thegraphpartitioning_b200.learned eval --weights gnn_weights.npz
+    python -m thegraphpartitioning_b200.learned train-move --init gnn_weights.npz --out gnn_weights.npz
+    python -m thegraphpartitioning_b200.learned eval --weights gnn_weights.npz --seeds 0,1,2
 """
 from __future__ import annotations
 
@@ -32,7 +40,7 @@ import time
 import numpy as np
 
 from . import GNN, partition, partition_learned, graphs as G
-from ._abi import GP_TR_MATCH, GP_TR_CONTRACT, GP_TR_LEVEL_DONE
+from ._abi import GP_TR_MATCH, GP_TR_CONTRACT, GP_TR_LEVEL_DONE, GP_TR_REFINE_ITER
 
 H, F0, MSG, ZD = 64, 4, 8, 4
 O_W1 = 0
@@ -43,8 +51,16 @@ O_B2 = O_W2 + H * (H + MSG)
 O_Z = O_B2 + H
 O_A = O_Z + ZD * H
 O_BETA = O_A + ZD
-NPARAM = O_BETA + 3
+O_ETA = O_BETA + 3          # common-neighbour coefficient
+NPARAM = O_BETA + 4
 FAMILIES = ("chung_lu", "rmat", "rgg", "er")
+# move-order head: W1[MH, MF] b1[MH] w2[MH] b2
+MH, MF = 16, 4
+MO_W1 = 0
+MO_B1 = MO_W1 + MH * MF
+MO_W2 = MO_B1 + MH
+MO_B2 = MO_W2 + MH
+MNPARAM = MO_B2 + 1
 
 
 def init_params(seed: int = 0) -> np.ndarray:
@@ -115,6 +131,79 @@ def level_samples(rowptr, colidx, k: int, seed: int = 0, imbalance: float = 0.03
         label = (p[src] == p[ci.long()]).to(torch.uint8)
         out.append((rp, ci, vw, ew, lvl, label))
     return out
+
+
+def move_samples(rowptr, colidx, k: int, seed: int = 0, imbalance: float = 0.03):
+    """(features float32[r, 4], labels uint8[r]) CUDA tensors: every
+    label-propagation candidate of the plain V-cycle, labelled 1 when it ends
+    its level in the part it proposed."""
+    import torch
+    dev = rowptr.device
+    _, _, ev = partition(rowptr, colidx, k, imbalance=imbalance, seed=seed,
+                         trace={GP_TR_CONTRACT, GP_TR_REFINE_ITER, GP_TR_LEVEL_DONE})
+    graphs = {0: (rowptr, None)}
+    steps, final = {}, {}
+    for e in ev:
+        if e["kind"] == GP_TR_CONTRACT:
+            graphs[e["level"] + 1] = (torch.from_numpy(e["rowptr"]).to(dev), torch.from_numpy(e["vwgt"]).to(dev))
+        elif e["kind"] == GP_TR_REFINE_ITER and e["mode"] == 0:
+            steps.setdefault(e["level"], []).append((e["a0"], e["a1"]))
+        elif e["kind"] == GP_TR_LEVEL_DONE:
+            final[e["level"]] = e["a0"]
+    feats, labels = [], []
+    for lvl, lst in steps.items():
+        rp, vw = graphs[lvl]
+        fin = final[lvl]
+        for dest, gain in lst:
+            cand = np.nonzero(dest >= 0)[0]
+            if len(cand) == 0:
+                continue
+            f = GNN.move_features(rp, torch.from_numpy(dest).to(dev), torch.from_numpy(gain).to(dev), vw, lvl)
+            idx = torch.from_numpy(cand).to(dev)
+            feats.append(f[idx])
+            labels.append(torch.from_numpy((fin[cand] == dest[cand]).astype(np.uint8)).to(dev))
+    if not feats:
+        return torch.zeros((0, 4), device=dev), torch.zeros(0, dtype=torch.uint8, device=dev)
+    return torch.cat(feats), torch.cat(labels)
+
+
+def build_move_dataset(count: int, seed: int = 0, device="cuda", log=None):
+    import torch
+    feats, labels, t0 = [], [], time.time()
+    for i in range(count):
+        spec = graph_spec(i, seed)
+        rp, ci = make_graph(spec, device)
+        k = min(spec["k"], max(2, (rp.numel() - 1) // 64))
+        f, y = move_samples(rp, ci, k, seed=spec["seed"])
+        feats.append(f)
+        labels.append(y)
+        if log and (i + 1) % 100 == 0:
+            log(f"graphs {i + 1}/{count}: {sum(x.shape[0] for x in feats)} candidates, {time.time() - t0:.1f}s")
+    return torch.cat(feats), torch.cat(labels)
+
+
+def train_move_head(model: GNN, feat, label, steps: int = 600, lr: float = 1e-2, log=None):
+    """Full-batch Adam on the candidate rows, cosine-decayed step size; returns
+    the loss before the first and after the last step."""
+    first = model.move_grad(feat, label)[0]
+    for t in range(steps):
+        cur = lr * 0.5 * (1 + math.cos(math.pi * t / max(steps, 1)))
+        loss = model.move_train_step(feat, label, lr=max(cur, lr * 0.02))
+        if log and t % 100 == 0:
+            log(f"move head step {t}: loss {loss:.4f}")
+    return first, model.move_grad(feat, label)[0]
+
+
+def move_init_params(seed: int = 0) -> np.ndarray:
+    """Head that starts as the plain (gain) order: hidden unit 0 copies the
+    signed log gain, the output is a positive multiple of it."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MNPARAM, dtype=np.float32)
+    p[MO_W1:MO_B1] = rng.normal(0, math.sqrt(2.0 / MF), MH * MF) * 0.1
+    p[MO_W1 + 0] = 1.0
+    p[MO_B1 + 0] = 0.5
+    p[MO_W2 + 0] = 4.0
+    return p
 
 
 def build_dataset(count: int, seed: int = 0, device="cuda", log=None):
@@ -226,8 +315,16 @@ def main(argv=None):
     t.add_argument("--out", default="gnn_weights.npz")
     t.add_argument("--init", default=None, help="start from these weights instead of a seeded init")
     t.add_argument("--tune-only", action="store_true", help="with --init: only re-tune prio_bits / max_level")
+    tm = sub.add_parser("train-move")
+    tm.add_argument("--init", required=True, help="model (edge scorer) to add the head to")
+    tm.add_argument("--graphs", type=int, default=400)
+    tm.add_argument("--steps", type=int, default=600)
+    tm.add_argument("--lr", type=float, default=1e-2)
+    tm.add_argument("--seed", type=int, default=0)
+    tm.add_argument("--out", default="gnn_weights.npz")
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=None)
+    e.add_argument("--seeds", default="0", help="partition seeds; the table reports each and their spread")
     e.add_argument("--graphs", default="rmat22,grid3d256")
     e.add_argument("--k", type=int, default=32)
     e.add_argument("--reps", type=int, default=2)
@@ -251,16 +348,58 @@ def main(argv=None):
         log(f"prio_bits = {model.prio_bits}, max_level = {model.max_level}")
         model.save(a.out)
         log(f"saved {a.out}")
+    elif a.cmd == "train-move":
+        model = GNN.load(a.init)
+        t0 = time.time()
+        feat, label = build_move_dataset(a.graphs, a.seed, log=log)
+        log(f"move dataset: {feat.shape[0]} candidates ({float(label.float().mean()):.3f} accepted), "
+            f"{time.time() - t0:.1f}s")
+        model.set_move_params(move_init_params(a.seed))
+        l0, l1 = train_move_head(model, feat, label, a.steps, a.lr, log=log)
+        log(f"move head loss {l0:.4f} -> {l1:.4f}")
+        del feat, label
+        torch.cuda.empty_cache()
+        # keep the head only when it lowers the validation cut
+        val = validation_set()
+        k = 32
+        ratios = {}
+        for use in (False, True):
+            saved = model.get_move_params()
+            if not use:
+                model.set_move_params(None)
+            logs = [math.log(max(partition_learned(rp, ci, k, model, fallback=False)[1]["cut"], 1) /
+                             max(partition(rp, ci, k)[1]["cut"], 1)) for rp, ci in val]
+            ratios[use] = math.exp(sum(logs) / len(logs))
+            if not use:
+                model.set_move_params(saved)
+        log(f"validation geometric-mean cut ratio vs plain: without head {ratios[False]:.4f}, "
+            f"with head {ratios[True]:.4f}")
+        if ratios[True] >= ratios[False]:
+            model.set_move_params(None)
+            log("head not kept")
+        model.save(a.out)
+        log(f"saved {a.out}")
     else:
         from . import default_gnn
         model = GNN.load(a.weights) if a.weights else default_gnn()
         res = {}
+        seeds = [int(x) for x in a.seeds.split(",")]
         for name in a.graphs.split(","):
             rp, ci = held_out(name)
-            r = evaluate(model, rp, ci, a.k, reps=a.reps)
-            r.update({"graph": name, "n": rp.numel() - 1, "undirected_edges": ci.numel() // 2, "k": a.k})
-            log(json.dumps(r))
-            res[name] = r
+            rows = []
+            for sd in seeds:
+                r = evaluate(model, rp, ci, a.k, seed=sd, reps=a.reps)
+                r.update({"graph": name, "seed": sd, "n": rp.numel() - 1, "undirected_edges": ci.numel() // 2,
+                          "k": a.k, "move_head": model.get_move_params() is not None})
+                log(json.dumps(r))
+                rows.append(r)
+            cr = [r["cut_ratio"] for r in rows]
+            pl = [r["cut_plain"] for r in rows]
+            res[name] = {"runs": rows, "cut_ratio_geomean": math.exp(sum(math.log(x) for x in cr) / len(cr)),
+                         "cut_ratio_min": min(cr), "cut_ratio_max": max(cr),
+                         "plain_seed_spread": max(pl) / max(min(pl), 1),
+                         "time_ratio_max": max(r["time_ratio"] for r in rows)}
+            log(json.dumps({k2: v for k2, v in res[name].items() if k2 != "runs"}))
             del rp, ci
             torch.cuda.empty_cache()
         if a.json:
