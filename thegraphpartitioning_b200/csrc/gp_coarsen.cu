@@ -577,8 +577,9 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // layout (row c at off[c]).  Every tier writes its unique entries at off[c]
 // (a bound on the row) and k_contract_copy packs them.  Tiers by row length d:
 //   A  d <= 128        one warp, 256-slot table in shared memory
-//   B  d <= 1024       one warp, 2048-slot table in shared memory
-//   C  d <= 4096       one CTA of 256 threads, two-phase (first position kept by
+//   A2 d <= 256        one warp, 512-slot table
+//   B  d <= 512        one warp, 1024-slot table (11 KB per warp: 20 warps per SM)
+//   C  d <= 4096       one CTA of 512 threads, two-phase (first position kept by
 //                      atomicMax of deg - j), 8192-slot table on chip
 //   C2 d <= 12288      the same with 1024 threads and a 16384-slot table (196 KB:
 //                      one CTA per SM; load factor at most 3/4)
@@ -588,8 +589,9 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 // block scan over per-thread contiguous segments.  The on-chip tables are
 // cleared once per CTA and afterwards only in the slots a row used.
 constexpr int TA_ROW = 128, TA_SLOTS = 256;
-constexpr int TB_ROW = 1024, TB_SLOTS = 2048, TB_WARPS = 4;
-constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 256;
+constexpr int TA2_ROW = 256, TA2_SLOTS = 512;
+constexpr int TB_ROW = 512, TB_SLOTS = 1024, TB_WARPS = 4;
+constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 512;
 constexpr int TC2_ROW = 12288, TC2_SLOTS = 16384, TC2_T = 1024;
 constexpr int TD_T = 1024;
 constexpr int32_t EMPTY_KEY = -1;
@@ -1093,14 +1095,19 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     memset_async(c, err, 0, sizeof(int32_t));
     {
         constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
+        constexpr size_t smA2 = 8 * warp_dedup_smem<TA2_ROW, TA2_SLOTS, int16_t>();
         constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
         auto kA = k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>;
+        auto kA2 = k_dedup_warp<TA2_ROW, TA2_SLOTS, 8, int16_t>;
         auto kB = k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>;
         kA<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, smA, c.s>>>(g, fine.cmap, mem, nc, 0, off, cdeg,
                                                                                   tci, tew, rowcnt);
         GP_LAUNCHED(c);
+        kA2<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, smA2, c.s>>>(g, fine.cmap, mem, nc, TA_ROW + 1,
+                                                                                    off, cdeg, tci, tew, rowcnt);
+        GP_LAUNCHED(c);
         kB<<<grid_for(nc * 32, TB_WARPS * 32, c.sm_count * c.ctas_per_sm), TB_WARPS * 32, smB, c.s>>>(
-            g, fine.cmap, mem, nc, TA_ROW + 1, off, cdeg, tci, tew, rowcnt);
+            g, fine.cmap, mem, nc, TA2_ROW + 1, off, cdeg, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
     k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listD, lcount);
@@ -1213,9 +1220,12 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
 // device (the cap is per kernel and shared by every thread of the process)
 void coarsen_smem_caps() {
     constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
+    constexpr size_t smA2 = 8 * warp_dedup_smem<TA2_ROW, TA2_SLOTS, int16_t>();
     constexpr size_t smB = TB_WARPS * warp_dedup_smem<TB_ROW, TB_SLOTS, int16_t>();
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TA_ROW, TA_SLOTS, 8, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smA));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TA2_ROW, TA2_SLOTS, 8, int16_t>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA2));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
