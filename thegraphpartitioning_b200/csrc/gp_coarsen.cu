@@ -583,6 +583,9 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 //                      atomicMax of deg - j), 8192-slot table on chip
 //   C2 d <= 12288      the same with 1024 threads and a 16384-slot table (196 KB:
 //                      one CTA per SM; load factor at most 3/4)
+//   C3 d <= 65536      one 1024-thread CTA, the C2 table in P = 2..8 passes: pass p
+//                      dedups the keys whose pass hash is p, first positions are
+//                      marked in a shared-memory bitmap of the whole walk
 //   D  longer          pieces of 64K entries, one CTA each, table in global memory
 // A and B insert 32 entries at a time in walk order (match_any leaders), so
 // new neighbours get consecutive ranks; C and D rank first positions with one
@@ -593,6 +596,7 @@ constexpr int TA2_ROW = 256, TA2_SLOTS = 512;
 constexpr int TB_ROW = 512, TB_SLOTS = 1024, TB_WARPS = 4;
 constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 512;
 constexpr int TC2_ROW = 12288, TC2_SLOTS = 16384, TC2_T = 1024;
+constexpr int TC3_ROW = 65536, TC3_KEYS = 12288;   // at most TC3_KEYS walk entries per pass on average
 constexpr int TD_T = 1024;
 constexpr int32_t EMPTY_KEY = -1;
 
@@ -743,11 +747,13 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
     return r;
 }
 
-// rows longer than TB_ROW: lists of the on-chip tiers C (<= TC_ROW) and C2
-// (<= TC2_ROW) and of tier D.  count[0] = rows of tier C, count[1] = rows of
-// tier D, count[2] = longest tier-D row, count[3] = rows of tier C2
+// rows longer than TB_ROW: lists of the on-chip tiers C (<= TC_ROW), C2
+// (<= TC2_ROW), C3 (<= TC3_ROW) and of tier D.  count[0] = rows of tier C,
+// count[1] = rows of tier D, count[2] = longest tier-D row, count[3] = rows of
+// tier C2, count[4] = rows of tier C3
 __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC,
-                            int32_t* __restrict__ listC2, int32_t* __restrict__ listD, int64_t* __restrict__ count) {
+                            int32_t* __restrict__ listC2, int32_t* __restrict__ listC3, int32_t* __restrict__ listD,
+                            int64_t* __restrict__ count) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = cdeg[c];
         if (d <= TB_ROW) continue;
@@ -757,6 +763,9 @@ __global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_
         } else if (d <= TC2_ROW) {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[3], 1ull);
             listC2[slot] = (int32_t)c;
+        } else if (d <= TC3_ROW) {
+            unsigned long long slot = atomicAdd((unsigned long long*)&count[4], 1ull);
+            listC3[slot] = (int32_t)c;
         } else {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[1], 1ull);
             listD[slot] = (int32_t)c;
@@ -898,6 +907,140 @@ __global__ void __launch_bounds__(T) k_dedup_cta_smem(DGraph g, const int32_t* _
         while (S < 2 * deg && S < SLOTS) { S <<= 1; ++lg; }
         cta_dedup<T>(g, cmap, walk_of(g, mem, c), off[c], deg, (int32_t)c, slot, wsum, hj, lg, words, tci, tew,
                      &cnt[c], sh, err);
+    }
+}
+
+// tier C3: one 1024-thread CTA per row of TC2_ROW < d <= TC3_ROW walk entries.
+// Pass 0 gathers the walk through cmap once and leaves the mapped ids and
+// weights in the row's range of the scratch arrays (key_at, w_at); passes
+// 1..P-1 read them from there (P = the power of two with d / P <= TC3_KEYS).
+// Pass p inserts only the keys whose pass hash is p into the 16384-slot table
+// (the same 64-bit slots as tier C: (key + 1) << 32 | (d - j), first position
+// kept by atomicMax, weights summed), then every used slot marks its first
+// position in a bitmap of the walk, leaves its weight sum at that position of
+// w_at (later passes never read the weights of another pass's keys), and is
+// cleared.  After the passes one block scan ranks
+// the marked positions and the keys are written in first-occurrence order, as
+// every other tier writes them.
+constexpr size_t tc3_smem() {
+    return (sizeof(unsigned long long) + sizeof(int32_t)) * TC2_SLOTS + sizeof(uint32_t) * 2 * (TC3_ROW / 32);
+}
+__device__ __forceinline__ uint32_t pass_of(int32_t key, int lgp) {
+    return lgp ? ((uint32_t)key * 0x85EBCA77u) >> (32 - lgp) : 0u;
+}
+__global__ void __launch_bounds__(TC2_T) k_dedup_multipass(DGraph g, const int32_t* __restrict__ cmap,
+                                                           const int32_t* __restrict__ mem,
+                                                           const int32_t* __restrict__ list, int64_t nlist,
+                                                           const int64_t* __restrict__ off,
+                                                           const int64_t* __restrict__ cdeg,
+                                                           int32_t* __restrict__ key_at, int32_t* __restrict__ w_at,
+                                                           int32_t* __restrict__ tci, int32_t* __restrict__ tew,
+                                                           int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+    constexpr int T = TC2_T, S = TC2_SLOTS, LG = 14;
+    static_assert((1 << LG) == S, "table size");
+    extern __shared__ __align__(16) unsigned char mp_raw[];
+    unsigned long long* slot = (unsigned long long*)mp_raw;            // S
+    int32_t* wsum = (int32_t*)(slot + S);                              // S
+    uint32_t* bits = (uint32_t*)(wsum + S);                            // TC3_ROW / 32
+    int32_t* wpre = (int32_t*)(bits + TC3_ROW / 32);                   // TC3_ROW / 32
+    __shared__ int32_t sh[33];
+    for (int i = threadIdx.x; i < S; i += T) { slot[i] = 0ull; wsum[i] = 0; }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = T / 32;
+    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
+        const int64_t c = list[li];
+        const int64_t deg = cdeg[c], o = off[c];
+        const int32_t self = (int32_t)c;
+        const Walk W = walk_of(g, mem, c);
+        const int64_t nwords = (deg + 31) / 32;
+        int lgp = 0;
+        while ((deg >> lgp) > TC3_KEYS) ++lgp;
+        for (int64_t i = threadIdx.x; i < nwords; i += T) bits[i] = 0u;
+        __syncthreads();
+        for (uint32_t pass = 0; pass < (1u << lgp); ++pass) {
+            for (int64_t base = 0; base < deg; base += 4 * T) {
+                int32_t cu[4], wt[4];
+                if (pass == 0) {
+                    // all four gathers in flight before the stores
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t j = base + q * T + threadIdx.x;
+                        cu[q] = self; wt[q] = 0;
+                        if (j < deg) walk_load(g, cmap, W, j, cu[q], wt[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t j = base + q * T + threadIdx.x;
+                        if (j < deg) { key_at[o + j] = cu[q]; w_at[o + j] = wt[q]; }
+                        if (cu[q] != self && pass_of(cu[q], lgp) != pass) cu[q] = self;
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t j = base + q * T + threadIdx.x;
+                        cu[q] = j < deg ? __ldcg(&key_at[o + j]) : self;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t j = base + q * T + threadIdx.x;
+                        if (cu[q] != self && pass_of(cu[q], lgp) != pass) cu[q] = self;
+                        wt[q] = cu[q] != self ? __ldcg(&w_at[o + j]) : 0;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (cu[q] == self) continue;
+                    const int64_t j = base + q * T + threadIdx.x;
+                    const unsigned long long val = ((unsigned long long)((uint32_t)cu[q] + 1u) << 32) | (uint32_t)(deg - j);
+                    const uint32_t tag = (uint32_t)cu[q] + 1u;
+                    uint32_t h = slot_hash(cu[q], LG);
+                    unsigned long long old = atomicCAS(&slot[h], 0ull, val);
+                    uint32_t probe = 1;
+                    while (old != 0ull && (uint32_t)(old >> 32) != tag && probe < (uint32_t)S) {
+                        h = (h + 1) & (S - 1);
+                        old = atomicCAS(&slot[h], 0ull, val);
+                        ++probe;
+                    }
+                    if (old != 0ull && (uint32_t)(old >> 32) != tag) { atomicExch(err, 1); continue; }
+                    if (old != 0ull && old < val) atomicMax(&slot[h], val);
+                    atomicAdd(&wsum[h], wt[q]);
+                }
+            }
+            __syncthreads();
+            // the pass's keys: mark first positions, park key and weight there, clear
+            for (int i = threadIdx.x; i < S; i += T) {
+                const unsigned long long v = slot[i];
+                if (!v) continue;
+                const int64_t j = deg - (int64_t)(uint32_t)v;
+                if (GP_IN(j, deg)) {
+                    atomicOr(&bits[j >> 5], 1u << (j & 31));
+                    w_at[o + j] = wsum[i];
+                }
+                slot[i] = 0ull;
+                wsum[i] = 0;
+            }
+            __syncthreads();
+        }
+        // ranks of the marked positions: contiguous word ranges per thread
+        const int64_t per = (nwords + T - 1) / T;
+        const int64_t w0 = (int64_t)threadIdx.x * per, w1 = w0 + per < nwords ? w0 + per : nwords;
+        int32_t mine = 0;
+        for (int64_t wi = w0; wi < w1; ++wi) mine += __popc(bits[wi]);
+        int32_t tot;
+        int32_t run = block_scan_excl(mine, sh, tot);
+        for (int64_t wi = w0; wi < w1; ++wi) { wpre[wi] = run; run += __popc(bits[wi]); }
+        __syncthreads();
+        const uint32_t lt = (1u << lane) - 1u;
+        for (int64_t wi = wid; wi < nwords; wi += nwarp) {
+            const uint32_t word = bits[wi];
+            if (!((word >> lane) & 1u)) continue;
+            const int64_t j = wi * 32 + lane;
+            const int32_t r = wpre[wi] + __popc(word & lt);
+            if (!GP_IN(r, deg)) continue;
+            tci[o + r] = key_at[o + j];
+            tew[o + r] = w_at[o + j];
+        }
+        if (threadIdx.x == 0) cnt[c] = tot;
+        __syncthreads();
     }
 }
 
@@ -1088,10 +1231,11 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
     int32_t* listC = c.tmp_alloc<int32_t>(nc);
     int32_t* listC2 = c.tmp_alloc<int32_t>(nc);
+    int32_t* listC3 = c.tmp_alloc<int32_t>(nc);
     int32_t* listD = c.tmp_alloc<int32_t>(nc);
-    int64_t* lcount = c.tmp_alloc<int64_t>(4);
+    int64_t* lcount = c.tmp_alloc<int64_t>(5);
     int32_t* err = c.tmp_alloc<int32_t>(1);
-    memset_async(c, lcount, 0, 4 * sizeof(int64_t));
+    memset_async(c, lcount, 0, 5 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
         constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
@@ -1110,11 +1254,12 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
             g, fine.cmap, mem, nc, TA2_ROW + 1, off, cdeg, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
-    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listD, lcount);
+    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listC3, listD, lcount);
     GP_LAUNCHED(c);
-    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 5 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
     c.sync();
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2], nC2 = c.h_pinned[3];
+    const int64_t nC3 = c.h_pinned[4];
     if (nC > 0) {
         // one CTA per row: the block scheduler balances rows of unequal length
         k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>
@@ -1128,6 +1273,13 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
             <<<(unsigned)std::min<int64_t>(nC2, (int64_t)c.sm_count * c.ctas_per_sm), TC2_T,
                cta_dedup_smem<TC2_SLOTS, TC2_ROW>(), c.s>>>(g, fine.cmap, mem, listC2, nC2, off, cdeg, tci, tew, rowcnt,
                                                             err);
+        GP_LAUNCHED(c);
+    }
+    if (nC3 > 0) {
+        // key and weight of each first occurrence are parked at its walk position
+        // in mapped / mw (free at these rows: only tier-D rows use them otherwise)
+        k_dedup_multipass<<<(unsigned)std::min<int64_t>(nC3, (int64_t)c.sm_count * c.ctas_per_sm), TC2_T, tc3_smem(),
+                            c.s>>>(g, fine.cmap, mem, listC3, nC3, off, cdeg, mapped, mw, tci, tew, rowcnt, err);
         GP_LAUNCHED(c);
     }
     if (nD > 0) {
@@ -1232,6 +1384,7 @@ void coarsen_smem_caps() {
                                  (int)cta_dedup_smem<TC_SLOTS, TC_ROW>()));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_dedup_smem<TC2_SLOTS, TC2_ROW>()));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_multipass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc3_smem()));
 }
 
 }  // namespace gp
