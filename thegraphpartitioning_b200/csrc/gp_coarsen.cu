@@ -241,7 +241,7 @@ __device__ __forceinline__ void match_tile(const MatchArgs& A, int64_t v) {
             }
         }
     }
-    group_argmax64(TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (lane & ~(TILE - 1))), bk, bid);
+    tile_argmax64<TILE>(bk, bid);
     const bool lead = tl == 0;
     if (MODE == 0) {
         if (lead && v >= 0) A.out[v] = valid ? bid : -1;

@@ -141,6 +141,33 @@ __device__ __forceinline__ void group_argmax64(uint32_t mask, uint64_t& k, int32
     k = ((uint64_t)mh << 32) | ml;
     id = (int32_t)mi;
 }
+// The same argmax and a sum over aligned groups of TILE lanes (TILE a power of
+// two <= 32; every lane of the warp calls them).  A group smaller than the
+// warp reduces with butterfly shuffles inside the group: a redux.sync whose
+// member mask differs between the lanes of one warp runs once per group.
+template <int TILE>
+__device__ __forceinline__ void tile_argmax64(uint64_t& k, int32_t& id) {
+    if constexpr (TILE == 32) {
+        group_argmax64(0xffffffffu, k, id);
+    } else {
+#pragma unroll
+        for (int o = TILE / 2; o > 0; o >>= 1) {
+            const uint64_t k2 = __shfl_xor_sync(0xffffffffu, k, o);
+            const int32_t i2 = __shfl_xor_sync(0xffffffffu, id, o);
+            if (k2 > k || (k2 == k && (uint32_t)i2 < (uint32_t)id)) { k = k2; id = i2; }
+        }
+    }
+}
+template <int TILE>
+__device__ __forceinline__ uint32_t tile_sum_u32(uint32_t x) {
+    if constexpr (TILE == 32) {
+        return __reduce_add_sync(0xffffffffu, x);
+    } else {
+#pragma unroll
+        for (int o = TILE / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        return x;
+    }
+}
 #endif
 // Four consecutive entries [e, e + 4) of a row [beg, end) of a CSR array
 // (column ids, weights or per-entry priorities), e a multiple of 4: one

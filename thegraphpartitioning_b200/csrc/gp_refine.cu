@@ -55,6 +55,22 @@ __device__ __forceinline__ void group_argmax_u32(uint32_t mask, uint64_t& bk, in
     bk = mh;
     bq = mh ? (int32_t)mq : -1;
 }
+// group_argmax_u32 over aligned groups of TILE lanes (see tile_argmax64)
+template <int TILE>
+__device__ __forceinline__ void tile_argmax_u32(uint64_t& bk, int32_t& bq, uint32_t h, int32_t q) {
+    if constexpr (TILE == 32) {
+        group_argmax_u32(0xffffffffu, bk, bq, h, q);
+    } else {
+        uint32_t kq = h ? (uint32_t)q : 0xffffffffu;
+#pragma unroll
+        for (int o = TILE / 2; o > 0; o >>= 1) {
+            const uint32_t h2 = __shfl_xor_sync(0xffffffffu, h, o), q2 = __shfl_xor_sync(0xffffffffu, kq, o);
+            if (h2 > h || (h2 == h && q2 < kq)) { h = h2; kq = q2; }
+        }
+        bk = h;
+        bq = h ? (int32_t)kq : -1;
+    }
+}
 __device__ __forceinline__ void argmax_u32(uint32_t& bh, int32_t& bq, uint32_t h, int32_t q) {
     if (h > bh || (h == bh && (uint32_t)q < (uint32_t)bq)) { bh = h; bq = q; }
 }
@@ -67,9 +83,11 @@ __device__ __forceinline__ bool lp_candidate(int64_t g, int64_t own, int32_t den
 // ------------------------------------------------------------------ k_conn
 // One unit of work per warp: 4 rows of bucket 0 (8 lanes each), or 1 row of
 // bucket 1, or 1 row of bucket 2; rows longer than kHeavyDeg take CTAs
-// [0, nheavy).  Buckets 0/1 keep their entries in registers and build the
-// connectivity histogram with match_any + redux.sync (no shared memory);
-// bucket 2 and heavy rows use a shared-memory histogram.
+// [0, nheavy).  Buckets 0/1 keep their entries in registers: a bucket-0 lane
+// sums the weights of its 8-lane tile's entries of the same part with seven
+// shuffles, a bucket-1 row adds its entries into the warp's shared-memory
+// histogram and reads its own part's bin back; bucket 2 and heavy rows build
+// the whole shared-memory histogram.
 // status: [S_CROSS] += directed cross weight; [S_MAXPW], [S_MODE], [S_LIGHT]
 // written by CTA 0; LP candidates are appended to clist[bucket] (any order:
 // each is evaluated on its own), with [S_NL0..S_NL2] their counts and
@@ -164,11 +182,15 @@ __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool ac
     return cand;
 }
 
-// rows of at most TILE entries, TILE lanes per row, 32/TILE rows per warp
+// rows of at most TILE entries, TILE lanes per row, 32/TILE rows per warp.
+// Every lane ends with the connectivity of the row to its entry's part; lanes
+// of the same part hold the same value, which the argmax (ties to the smaller
+// part) does not mind.  hist: the warp's k zeroed bins (TILE == 32 only; left
+// zeroed).
 template <int TILE, class PT>
 __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
-                                          int list_id, int64_t& acc) {
-    const int lane = threadIdx.x & 31, tl = lane & (TILE - 1), tix = lane / TILE;
+                                          int list_id, int32_t* hist, int64_t& acc) {
+    const int lane = threadIdx.x & 31, tl = lane & (TILE - 1);
     int64_t beg = 0, end = 0;
     int32_t p = -1;
     bool active = false;
@@ -181,16 +203,33 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
     if (has) { q = gpart<PT>(A.pc, __ldcs(&A.g.ci[e]), A.g.n); w = A.g.ew ? __ldcs(&A.g.ew[e]) : 1; }
-    const uint32_t tmask = TILE == 32 ? 0xffffffffu : (((1u << TILE) - 1u) << (tix * TILE));
-    const int32_t cross = (int32_t)__reduce_add_sync(tmask, (has && q != p) ? (uint32_t)w : 0u);
-    const int32_t tot = (int32_t)__reduce_add_sync(tmask, (uint32_t)w);
-    const uint32_t key = has ? (((uint32_t)tix << 20) | (uint32_t)q) : (0x80000000u | (uint32_t)lane);
-    const uint32_t peers = __match_any_sync(0xffffffffu, key);
-    const uint32_t connq = __reduce_add_sync(peers, (uint32_t)w);
-    const bool lead = has && lane == __ffs(peers) - 1;
+    const int32_t cross = (int32_t)tile_sum_u32<TILE>((has && q != p) ? (uint32_t)w : 0u);
+    const int32_t tot = (int32_t)tile_sum_u32<TILE>((uint32_t)w);
+    uint32_t connq = 0;
+    if constexpr (TILE == 32) {
+        if (active) {  // one row per warp: uniform
+            const bool in = has && q != p && GP_IN(q, A.k);   // the own part's bin is not needed
+            if (in) atomicAdd(&hist[q], w);
+            __syncwarp();
+            if (in) connq = (uint32_t)hist[q];
+            __syncwarp();
+            if (in) hist[q] = 0;
+            __syncwarp();
+        }
+    } else {
+        const int32_t qk = has ? q : -1;
+        connq = has ? (uint32_t)w : 0u;
+#pragma unroll
+        for (int d = 1; d < TILE; ++d) {
+            const int src = (lane & ~(TILE - 1)) | ((tl + d) & (TILE - 1));
+            const int32_t q2 = __shfl_sync(0xffffffffu, qk, src);
+            const int32_t w2 = __shfl_sync(0xffffffffu, w, src);
+            if (has && q2 == q) connq += (uint32_t)w2;
+        }
+    }
     uint64_t bk;
     int32_t bq;
-    group_argmax_u32(tmask, bk, bq, (active && lead && q != p && (mode != MODE_RB || !over[q])) ? connq : 0u, q);
+    tile_argmax_u32<TILE>(bk, bq, (active && has && q != p && (mode != MODE_RB || !over[q])) ? connq : 0u, q);
     bool take = false;
     if (tl == 0 && v >= 0) {
         acc += cross;
@@ -427,10 +466,10 @@ __global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
             if (u < U2) {
                 conn_warp<PT>(A, A.bucket[2][u], mode, over, light, hist, acc);
             } else if (u < U2 + U1) {
-                conn_tile<kTile32, PT>(A, A.bucket[1][u - U2], mode, over, light, 1, acc);
+                conn_tile<kTile32, PT>(A, A.bucket[1][u - U2], mode, over, light, 1, hist, acc);
             } else {
                 const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8, PT>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, acc);
+                conn_tile<kTile8, PT>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, hist, acc);
             }
         }
     }
@@ -1127,10 +1166,11 @@ __device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
         int32_t* hist = s_hist + w * k;
         for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
             if (u < U2) conn_warp<int32_t>(CA, R.bucket[2][u], dmode, s_over, light, hist, acc);
-            else if (u < U2 + U1) conn_tile<kTile32, int32_t>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, acc);
+            else if (u < U2 + U1) conn_tile<kTile32, int32_t>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, hist, acc);
             else {
                 const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8, int32_t>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, acc);
+                conn_tile<kTile8, int32_t>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, hist,
+                                           acc);
             }
         }
         acc = warp_sum(acc);
