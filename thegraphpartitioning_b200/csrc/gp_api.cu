@@ -325,6 +325,8 @@ void vc_begin(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t see
     B.best_pw = c.keep_alloc<int64_t>(k);
     B.status = c.keep_alloc<int64_t>(S_NSLOTS);
     for (int b = 0; b < 3; ++b) B.clist[b] = c.keep_alloc<int32_t>(n0);
+    B.wfirst_cap = conn_max_warps(c) + 1;
+    B.wfirst = c.keep_alloc<int64_t>(B.wfirst_cap);
     int64_t hmax = 1;
     for (const Level& l : lv) hmax = std::max(hmax, l.nheavy);
     B.hhist = c.keep_alloc<int32_t>(hmax * k);

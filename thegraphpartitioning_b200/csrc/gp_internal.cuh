@@ -110,6 +110,8 @@ struct RefineBufs {
     int64_t* best_pw = nullptr;   // k
     int64_t* status = nullptr;    // 16
     int32_t* clist[3] = {nullptr, nullptr, nullptr};   // LP candidates by degree bucket
+    int64_t* wfirst = nullptr;    // first light unit of each warp of the connectivity pass (+ end)
+    int64_t wfirst_cap = 0;       // its length
     // accumulators of heavy rows split over several CTAs (zero between uses)
     int32_t* hhist = nullptr;     // nheavy_max * k connectivity sums
     int64_t* hsum = nullptr;      // nheavy_max * 2: cross, total (conn) / gain (afterburner)
@@ -204,6 +206,7 @@ int initial_partition(Ctx& c, const Level& L, const Params& P, int32_t* part_out
 
 // gp_refine.cu
 int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr);
+int64_t conn_max_warps(const Ctx& c);   // most light warps a connectivity pass launches
 void project(Ctx& c, const Level& fine, const int32_t* part_coarse, int32_t* part_fine);
 void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* pw);
 void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw);

@@ -110,8 +110,7 @@ struct ConnArgs {
     int64_t nitems;
     const int32_t* bucket[3];
     int64_t nbucket[3];
-    const int64_t* unit_cost;   // prefix of unit costs (nunits + 1)
-    int64_t nunits;
+    const int64_t* wfirst;      // first light unit of each light warp, and the end (nw + 1)
     int32_t* dest;
     int32_t* gain;
     int32_t* part_next;         // label propagation: part and cleared lock copied here for the
@@ -449,19 +448,9 @@ __global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
     } else {
         int32_t* hist = hist_all + w * k;
         const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * RT + threadIdx.x) >> 5;
-        const int64_t nw = ((int64_t)(gridDim.x - A.nitems) * RT) >> 5;
         const int64_t U2 = A.nbucket[2], U1 = A.nbucket[1];
-        // contiguous units of equal total cost: [first unit with prefix >= wid*T/nw, ...)
-        const int64_t T = A.unit_cost[A.nunits];
-        auto first_unit = [&](int64_t target) {
-            int64_t lo = 0, hi = A.nunits;
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (A.unit_cost[mid] < target) lo = mid + 1; else hi = mid;
-            }
-            return lo;
-        };
-        const int64_t u0 = first_unit((T * wid) / nw), u1 = first_unit((T * (wid + 1)) / nw);
+        // contiguous units of equal total cost (k_warp_bounds)
+        const int64_t u0 = A.wfirst[wid], u1 = A.wfirst[wid + 1];
         for (int64_t u = u0; u < u1; ++u) {
             if (u < U2) {
                 conn_warp<PT>(A, A.bucket[2][u], mode, over, light, hist, acc);
@@ -1157,7 +1146,7 @@ __device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
         CA.part = part; CA.lock = lock; CA.pw = s_pw; CA.heavy = nullptr; CA.item_row = nullptr;
         CA.item_beg = nullptr; CA.item_end = nullptr; CA.row_items = nullptr; CA.nitems = 0;
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = R.bucket[b]; CA.nbucket[b] = R.nbucket[b]; CA.clist[b] = R.clist[b]; }
-        CA.unit_cost = nullptr; CA.nunits = 0;
+        CA.wfirst = nullptr;
         CA.dest = R.dest; CA.gain = R.gain; CA.status = R.status;
         CA.part_next = nullptr; CA.lock_next = nullptr;
         CA.pc = part; CA.pc_next = nullptr;
@@ -1499,6 +1488,25 @@ __global__ void k_compact_part(int64_t n, const int32_t* __restrict__ part, void
         store_pc(pc, pcb, v, part[v]);
 }
 
+int64_t conn_max_warps(const Ctx& c) { return (int64_t)c.sm_count * c.ctas_per_sm * RW; }
+
+// light warp t of a connectivity pass over nw warps takes the units
+// [first unit with cost prefix >= T * t / nw, the same for t + 1), T the total
+// cost: contiguous ranges of equal cost, the same for every pass of a level
+__global__ void k_warp_bounds(const int64_t* __restrict__ cost, int64_t nunits, int64_t nw,
+                              int64_t* __restrict__ out) {
+    const int64_t T = cost[nunits];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= nw; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t target = (T * t) / nw;
+        int64_t lo = 0, hi = nunits;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (cost[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        out[t] = lo;
+    }
+}
+
 int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int level, const Tracer& tr) {
     if (cta_refine_ok(L, P)) return refine_level_cta(c, L, P, B, level, tr);
     const DGraph& g = L.g;
@@ -1516,8 +1524,14 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
     const int kpad = (k + 15) & ~15;
     const size_t conn_smem = kpad + sizeof(int32_t) * RW * k;
     // at most 1024 + 32 * GP_MAX_K bytes: below the 48 KB default, no attribute needed
-    const int light_blocks = grid_for(n * 32, RT, c.sm_count * c.ctas_per_sm);
+    const int light_blocks = (int)std::min<int64_t>(grid_for(n * 32, RT, c.sm_count * c.ctas_per_sm),
+                                                    (B.wfirst_cap - 1) / RW);
     const int grid = (int)L.nitems + light_blocks;
+    {
+        const int64_t nw = (int64_t)light_blocks * RW;
+        k_warp_bounds<<<grid_for(nw + 1, 256), 256, 0, c.s>>>(L.unit_cost, L.nunits, nw, B.wfirst);
+        GP_LAUNCHED(c);
+    }
     int64_t best_cut = 0, best_mp = 0;
     int stall = 0, rb_streak = 0, steps = 0, last_mode = 0;
     int64_t prev_moves = -1;
@@ -1532,7 +1546,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         CA.item_row = L.item_row; CA.item_beg = L.item_beg; CA.item_end = L.item_end; CA.row_items = L.row_items;
         CA.nitems = L.nitems; CA.hhist = B.hhist; CA.hsum = B.hsum; CA.hdone = B.hdone;
         for (int b = 0; b < 3; ++b) { CA.bucket[b] = L.bucket[b]; CA.nbucket[b] = L.nbucket[b]; CA.clist[b] = B.clist[b]; }
-        CA.unit_cost = L.unit_cost; CA.nunits = L.nunits;
+        CA.wfirst = B.wfirst;
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
         CA.part_next = B.part_next; CA.lock_next = B.lock_next;   // the LP step's starting copy
         CA.pc = B.pc; CA.pc_next = B.pc_next;
