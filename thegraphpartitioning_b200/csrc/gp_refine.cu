@@ -181,23 +181,59 @@ __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool ac
     return cand;
 }
 
+// one row of the connectivity pass: id (-1: none), entry range, part, and
+// whether it looks for a move in this mode
+struct ConnRow {
+    int64_t beg, end;
+    int32_t v, p;
+    bool active;
+};
+__device__ __forceinline__ ConnRow conn_row(const ConnArgs& A, int64_t v, int mode, const uint8_t* over) {
+    ConnRow r;
+    r.v = (int32_t)v; r.beg = 0; r.end = 0; r.p = -1; r.active = false;
+    if (v >= 0) {
+        r.beg = A.g.rp[v]; r.end = A.g.rp[v + 1];
+        r.p = A.part[v];
+        r.active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[r.p]);
+    }
+    return r;
+}
+// shared-memory copy of a ConnRow (pa: part, bit 31 = active)
+struct ConnRowS {
+    int64_t beg, end;
+    int32_t v, pa;
+};
+__device__ __forceinline__ ConnRowS conn_stage(const ConnRow& r) {
+    ConnRowS s;
+    s.beg = r.beg; s.end = r.end; s.v = r.v;
+    s.pa = (int32_t)((uint32_t)r.p | (r.active ? 0x80000000u : 0u));
+    return s;
+}
+__device__ __forceinline__ ConnRow conn_unstage(const ConnRowS& s) {
+    ConnRow r;
+    r.beg = s.beg; r.end = s.end; r.v = s.v;
+    r.p = s.v >= 0 ? (int32_t)((uint32_t)s.pa & 0x7fffffffu) : -1;
+    r.active = s.v >= 0 && s.pa < 0;
+    return r;
+}
+// the LP candidate list and its count slot of bucket b
+__device__ __forceinline__ int64_t* conn_list_count(const ConnArgs& A, int b) {
+    return &A.status[b == 0 ? S_NL0 : (b == 1 ? S_NL1 : S_NL2)];
+}
+
 // rows of at most TILE entries, TILE lanes per row, 32/TILE rows per warp.
 // Every lane ends with the connectivity of the row to its entry's part; lanes
 // of the same part hold the same value, which the argmax (ties to the smaller
 // part) does not mind.  hist: the warp's k zeroed bins (TILE == 32 only; left
-// zeroed).
+// zeroed).  Returns true on the row's first lane when the row is an LP
+// candidate (the caller appends it).
 template <int TILE, class PT>
-__device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
-                                          int list_id, int32_t* hist, int64_t& acc) {
+__device__ __forceinline__ bool conn_tile(const ConnArgs& A, const ConnRow& R, int mode, const uint8_t* over,
+                                          int32_t light, int32_t* hist, int64_t& acc) {
     const int lane = threadIdx.x & 31, tl = lane & (TILE - 1);
-    int64_t beg = 0, end = 0;
-    int32_t p = -1;
-    bool active = false;
-    if (v >= 0) {
-        beg = A.g.rp[v]; end = A.g.rp[v + 1];
-        p = A.part[v];
-        active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
-    }
+    const int64_t v = R.v, beg = R.beg, end = R.end;
+    const int32_t p = R.p;
+    const bool active = R.active;
     const int64_t e = beg + tl;
     const bool has = v >= 0 && e < end;
     int32_t q = -1, w = 0;
@@ -233,10 +269,8 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
     if (tl == 0 && v >= 0) {
         acc += cross;
         take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
-        if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
-    warp_push(take, (int32_t)v, A.clist[list_id], &A.status[S_NL0 + (list_id == 0 ? 0 : (list_id == 1 ? 1 : 3))],
-              A.g.n);
+    return take;
 }
 
 // bucket 2: one row per warp, shared-memory histogram.  The row is swept
@@ -248,12 +282,12 @@ __device__ __forceinline__ void conn_tile(const ConnArgs& A, int64_t v, int mode
 // non-zero connection).
 constexpr int kBinsK = 256;
 template <class PT>
-__device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode, const uint8_t* over, int32_t light,
-                                          int32_t* hist, int64_t& acc) {
+__device__ __forceinline__ bool conn_warp(const ConnArgs& A, const ConnRow& R, int mode, const uint8_t* over,
+                                          int32_t light, int32_t* hist, int64_t& acc) {
     const int lane = threadIdx.x & 31;
-    const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
-    const int32_t p = A.part[v];
-    const bool active = (mode == MODE_LP && !A.lock[v]) || (mode == MODE_RB && over[p]);
+    const int64_t v = R.v, beg = R.beg, end = R.end;
+    const int32_t p = R.p;
+    const bool active = R.active;
     int32_t cross = 0, tot = 0;
     // 128 entries per sweep, four consecutive ones per lane (16-byte loads)
     const bool v4 = aligned16(A.g.ci) && aligned16(A.g.ew);
@@ -310,9 +344,14 @@ __device__ __forceinline__ void conn_warp(const ConnArgs& A, int64_t v, int mode
     if (lane == 0) {
         acc += cross;
         take = conn_decide<PT>(A, mode, active, v, p, tot, cross, bk, bq, light);
-        if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(end - beg));
     }
-    warp_push(take, (int32_t)v, A.clist[2], &A.status[S_NL2], A.g.n);
+    return take;
+}
+
+// append a row decided by conn_tile / conn_warp to list b at once
+__device__ __forceinline__ void conn_push_now(const ConnArgs& A, bool take, const ConnRow& R, int b) {
+    if (take) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)(R.end - R.beg));
+    warp_push(take, R.v, A.clist[b], conn_list_count(A, b), A.g.n);
 }
 
 template <class PT>
@@ -328,6 +367,7 @@ __global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
     __shared__ int32_t s_q[RW];
     __shared__ int64_t s_maxpw;
     __shared__ int32_t s_light;
+    __shared__ ConnRowS s_rows[RT];   // light warps: 32 staged rows each
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 
     // over flags, heaviest part, lightest non-overweight part (ties: lower id)
@@ -447,20 +487,62 @@ __global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
         }
     } else {
         int32_t* hist = hist_all + w * k;
+        ConnRowS* rows = s_rows + w * 32;
         const int64_t wid = ((int64_t)(blockIdx.x - A.nitems) * RT + threadIdx.x) >> 5;
         const int64_t U2 = A.nbucket[2], U1 = A.nbucket[1];
-        // contiguous units of equal total cost (k_warp_bounds)
+        // contiguous units of equal total cost (k_warp_bounds), taken 8 at a
+        // time: lane l first fetches row slot l (unit l / 4; its row, or the
+        // (l % 4)-th row of a group of 4), so the list and row-header loads of
+        // 8 units are in flight together; the candidates of the 8 units are
+        // appended together afterwards (one atomic per list present)
         const int64_t u0 = A.wfirst[wid], u1 = A.wfirst[wid + 1];
-        for (int64_t u = u0; u < u1; ++u) {
-            if (u < U2) {
-                conn_warp<PT>(A, A.bucket[2][u], mode, over, light, hist, acc);
-            } else if (u < U2 + U1) {
-                conn_tile<kTile32, PT>(A, A.bucket[1][u - U2], mode, over, light, 1, hist, acc);
-            } else {
-                const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8, PT>(A, i < A.nbucket[0] ? A.bucket[0][i] : -1, mode, over, light, 0, hist, acc);
+        int64_t cdeg = 0;   // degree sum of this lane's candidates
+        for (int64_t ub = u0; ub < u1; ub += 8) {
+            const int nu = (int)(u1 - ub < 8 ? u1 - ub : 8);
+            {
+                const int64_t u = ub + (lane >> 2);
+                const int sub = lane & 3;
+                int64_t v = -1;
+                if (u < ub + nu) {
+                    if (u < U2) { if (sub == 0) v = A.bucket[2][u]; }
+                    else if (u < U2 + U1) { if (sub == 0) v = A.bucket[1][u - U2]; }
+                    else {
+                        const int64_t i = (u - U2 - U1) * 4 + sub;
+                        if (i < A.nbucket[0]) v = A.bucket[0][i];
+                    }
+                }
+                rows[lane] = conn_stage(conn_row(A, v, mode, over));
             }
+            __syncwarp();
+            uint32_t takes = 0;   // bit s: row slot s is a candidate
+            for (int j = 0; j < nu; ++j) {
+                const int64_t u = ub + j;
+                if (u < U2) {
+                    const bool t = conn_warp<PT>(A, conn_unstage(rows[4 * j]), mode, over, light, hist, acc);
+                    takes |= (__ballot_sync(0xffffffffu, t) & 1u) << (4 * j);
+                } else if (u < U2 + U1) {
+                    const bool t = conn_tile<kTile32, PT>(A, conn_unstage(rows[4 * j]), mode, over, light, hist, acc);
+                    takes |= (__ballot_sync(0xffffffffu, t) & 1u) << (4 * j);
+                } else {
+                    const bool t = conn_tile<kTile8, PT>(A, conn_unstage(rows[4 * j + (lane >> 3)]), mode, over, light,
+                                                         hist, acc);
+                    const uint32_t b = __ballot_sync(0xffffffffu, t);   // lanes 0, 8, 16, 24
+                    takes |= ((b & 1u) | ((b >> 7) & 2u) | ((b >> 14) & 4u) | ((b >> 21) & 8u)) << (4 * j);
+                }
+            }
+            {
+                const bool t = (takes >> lane) & 1u;
+                const ConnRowS rs = rows[lane];
+                const int64_t u = ub + (lane >> 2);
+                const int lb = u < U2 ? 2 : (u < U2 + U1 ? 1 : 0);
+                if (t) cdeg += rs.end - rs.beg;
+#pragma unroll
+                for (int b = 0; b < 3; ++b) warp_push(t && lb == b, rs.v, A.clist[b], conn_list_count(A, b), A.g.n);
+            }
+            __syncwarp();
         }
+        cdeg = warp_sum(cdeg);
+        if (lane == 0 && cdeg) atomicAdd((unsigned long long*)&A.status[S_CDEG], (unsigned long long)cdeg);
     }
     acc = warp_sum(acc);
     __syncthreads();
@@ -1154,12 +1236,16 @@ __device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
         int64_t acc = 0;
         int32_t* hist = s_hist + w * k;
         for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
-            if (u < U2) conn_warp<int32_t>(CA, R.bucket[2][u], dmode, s_over, light, hist, acc);
-            else if (u < U2 + U1) conn_tile<kTile32, int32_t>(CA, R.bucket[1][u - U2], dmode, s_over, light, 1, hist, acc);
-            else {
+            if (u < U2) {
+                const ConnRow r = conn_row(CA, R.bucket[2][u], dmode, s_over);
+                conn_push_now(CA, conn_warp<int32_t>(CA, r, dmode, s_over, light, hist, acc), r, 2);
+            } else if (u < U2 + U1) {
+                const ConnRow r = conn_row(CA, R.bucket[1][u - U2], dmode, s_over);
+                conn_push_now(CA, conn_tile<kTile32, int32_t>(CA, r, dmode, s_over, light, hist, acc), r, 1);
+            } else {
                 const int64_t i = (u - U2 - U1) * 4 + (lane >> 3);
-                conn_tile<kTile8, int32_t>(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over, light, 0, hist,
-                                           acc);
+                const ConnRow r = conn_row(CA, i < R.nbucket[0] ? R.bucket[0][i] : -1, dmode, s_over);
+                conn_push_now(CA, conn_tile<kTile8, int32_t>(CA, r, dmode, s_over, light, hist, acc), r, 0);
             }
         }
         acc = warp_sum(acc);
