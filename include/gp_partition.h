@@ -81,10 +81,10 @@ typedef struct gp_options {
                                    identical for every value (autotuner knob)          */
     int32_t heavy_deg;          /* rows longer than this many entries are scanned by whole
                                    CTAs (8 warps), shorter ones by one warp or a lane
-                                   group (0: 2048; 64..65536); results are identical
+                                   group (0: 4096; 64..65536); results are identical
                                    for every value (autotuner knob; the learned V-cycle
-                                   always uses the defaults of this and item_len)       */
-    int32_t item_len;           /* entries of one CTA's piece of a long row (0: 16384;
+                                   always uses 2048 and an item_len of 16384)          */
+    int32_t item_len;           /* entries of one CTA's piece of a long row (0: 32768;
                                    heavy_deg..1048576); results are identical (autotuner
                                    knob)                                                */
 } gp_options;

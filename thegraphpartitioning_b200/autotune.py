@@ -45,8 +45,8 @@ def _sample(n_graphs: int, costs, size: int):
 
 
 def autotune_batch(graphs, ks, imbalances=0.03, seeds=0, sample: int = 256, reps: int = 1,
-                   workers=None, small_level_n=(0, 2048), ctas_per_sm=(8, 64), heavy_deg=(2048,),
-                   item_len=(16384,), log=None):
+                   workers=None, small_level_n=(0, 2048), ctas_per_sm=(8, 64), heavy_deg=(4096,),
+                   item_len=(32768,), log=None):
     """Time every (workers, small_level_n, ctas_per_sm, heavy_deg, item_len)
     combination on a sample of the batch (after one warm-up call each) and
     return the fastest: {"workers", "options", "seconds", "table"}.  The sample
@@ -89,8 +89,8 @@ def autotune_batch(graphs, ks, imbalances=0.03, seeds=0, sample: int = 256, reps
 
 
 def autotune_graph(rowptr, colidx, k: int, imbalance: float = 0.03, seed: int = 0, vwgt=None, ewgt=None,
-                   ctas_per_sm=(16, 32, 64, 96), small_level_n=(0,), heavy_deg=(1024, 2048, 8192),
-                   item_len=(16384, 65536), reps: int = 1, log=None):
+                   ctas_per_sm=(16, 32, 64, 96), small_level_n=(0,), heavy_deg=(2048, 4096, 8192),
+                   item_len=(16384, 32768, 65536), reps: int = 1, log=None):
     """Time full partitions of one graph (CUDA tensors) for every combination
     of the grid knobs, by the device time the library reports, and return the
     fastest: {"options", "ms", "table"}."""

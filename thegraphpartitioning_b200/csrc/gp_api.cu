@@ -578,12 +578,12 @@ int gp_partition_learned_device(int64_t n, const int64_t* d_rowptr, const int32_
         g.ci = d_colidx; g.ew = d_ewgt; g.vw = d_vwgt;
         Tracer tr; tr.fn = trace; tr.user = trace_user;
         // the scorer's float sums follow the row layout, so the learned
-        // V-cycle keeps the default heavy-row threshold and piece length
+        // V-cycle uses one fixed heavy-row threshold and piece length
         gp_options lopt;
         if (opt) lopt = *opt;
         else { memset(&lopt, 0, sizeof lopt); lopt.version = GP_OPTIONS_VERSION; }
-        lopt.heavy_deg = 0;
-        lopt.item_len = 0;
+        lopt.heavy_deg = kLearnedHeavyDeg;
+        lopt.item_len = kLearnedItemLen;
         // the move-order head runs in the multi-kernel refinement loop only
         if (gnn_has_move_head(model)) lopt.small_level_n = 0;
         opt = &lopt;

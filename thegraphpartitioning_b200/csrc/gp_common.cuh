@@ -287,8 +287,11 @@ inline int grid_for(int64_t items, int per_block, int cap = 148 * 16) {
     if (g > cap) g = cap;
     return (int)g;
 }
-constexpr int kHeavyDeg = 2048;   // default: rows longer than this take whole CTAs (gp_options.heavy_deg)
-constexpr int kItemLen = 16384;   // default: entries of one CTA item of a long row (gp_options.item_len)
+constexpr int kHeavyDeg = 4096;   // default: rows longer than this take whole CTAs (gp_options.heavy_deg)
+constexpr int kItemLen = 32768;   // default: entries of one CTA item of a long row (gp_options.item_len)
+// the learned V-cycle's fixed row layout (its scorer's float sums follow it)
+constexpr int kLearnedHeavyDeg = 2048;
+constexpr int kLearnedItemLen = 16384;
 
 // ---------------------------------------------------------------- primitives (gp_prims.cu)
 // exclusive scan; out may alias in; returns total on the host if total_out != nullptr
