@@ -1192,16 +1192,73 @@ __global__ void k_td_rows(const int32_t* __restrict__ list, int64_t n, const int
 }
 
 // warp per coarse row: temporary (walk-bound offsets) -> final CSR
-__global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, const int64_t* __restrict__ off,
+// Packs every row's deduplicated entries (crp[c + 1] - crp[c] of them at
+// walk offset off[c] of tci / tew) into the coarse CSR.  The output is cut
+// into slices of CP_SLICE entries, one warp each: the warp finds the row
+// holding its first entry by binary search over crp, then keeps a window of
+// 32 consecutive rows (start and source offset, one row per lane); the row of
+// an output position is the last window row starting at or before it (five
+// shuffle steps).  Eight groups of 32 entries are loaded before any is stored.
+constexpr int64_t CP_SLICE = 16384;
+__device__ __forceinline__ int64_t cp_source(int64_t oi, int64_t s, int64_t src) {
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int64_t sv = __shfl_sync(0xffffffffu, s, l + step);
+        if (sv <= oi) l += step;
+    }
+    return __shfl_sync(0xffffffffu, src, l) + (oi - __shfl_sync(0xffffffffu, s, l));
+}
+__global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, int64_t cm, const int64_t* __restrict__ off,
                                                        const int64_t* __restrict__ crp, const int32_t* __restrict__ tci,
                                                        const int32_t* __restrict__ tew, int32_t* __restrict__ ci,
                                                        int32_t* __restrict__ ew) {
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = wid; c < nc; c += nw) {
-        const int64_t src = off[c], dst = crp[c], len = crp[c + 1] - crp[c];
-        for (int64_t i = lane; i < len; i += 32) { ci[dst + i] = tci[src + i]; ew[dst + i] = tew[src + i]; }
+    const int64_t nslice = (cm + CP_SLICE - 1) / CP_SLICE;
+    for (int64_t sl = wid; sl < nslice; sl += nw) {
+        const int64_t o0 = sl * CP_SLICE, o1 = o0 + CP_SLICE < cm ? o0 + CP_SLICE : cm;
+        int64_t lo = 0, hi = nc - 1;   // last row with crp[row] <= o0
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (crp[mid] <= o0) lo = mid; else hi = mid - 1;
+        }
+        int64_t cb = lo, s = 0, src = 0, wend = 0;
+        auto window = [&]() {   // rows cb .. cb + 31; wend = first output entry past them
+            const int64_t r = cb + lane;
+            s = r < nc ? crp[r] : cm;
+            src = r < nc ? off[r] : 0;
+            wend = crp[cb + 32 < nc ? cb + 32 : nc];
+        };
+        window();
+        int64_t o = o0;
+        while (o < o1) {
+            const int64_t lim = o1 < wend ? o1 : wend;
+            if (o + 256 <= lim) {
+                int32_t a[8], b[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int64_t p = cp_source(o + 32 * q + lane, s, src);
+                    a[q] = __ldcs(&tci[p]);
+                    b[q] = __ldcs(&tew[p]);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    ci[o + 32 * q + lane] = a[q];
+                    ew[o + 32 * q + lane] = b[q];
+                }
+                o += 256;
+            } else if (o < lim) {
+                const int64_t oi = o + lane;
+                const int64_t p = cp_source(oi, s, src);
+                if (oi < lim) { ci[oi] = tci[p]; ew[oi] = tew[p]; }
+                o = o + 32 < lim ? o + 32 : lim;
+            } else {
+                cb += 32;   // o >= wend: o lies in a later row
+                window();
+            }
+        }
     }
 }
 
@@ -1354,7 +1411,8 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     if ((int32_t)c.h_pinned[1] != 0) throw GpError(GP_EINTERNAL, "contraction hash table overflow");
     int32_t* cci = c.keep_alloc<int32_t>(mc);
     int32_t* cew = c.keep_alloc<int32_t>(mc);
-    k_contract_copy<<<grid_for(nc * 32, 256, c.sm_count * c.ctas_per_sm), 256, 0, c.s>>>(nc, off, crp, tci, tew, cci, cew);
+    k_contract_copy<<<grid_for((mc + CP_SLICE - 1) / CP_SLICE * 32, 256, c.sm_count * c.ctas_per_sm), 256, 0, c.s>>>(
+        nc, mc, off, crp, tci, tew, cci, cew);
     GP_LAUNCHED(c);
     // rows read twice (count and rank for long rows), cmap gathered per entry,
     // unique entries written to the temporary and copied once

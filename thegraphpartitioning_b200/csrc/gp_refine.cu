@@ -625,17 +625,17 @@ __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* 
     if (tl == 0 && v >= 0 && t >= 0) ab_commit<PT>(A, v, p, d, delta, moves);
 }
 
-// one candidate row of 33..kHeavyDeg entries per warp, 128 entries per sweep
+// this thread's part (thread t of nt) of the ab_term sum over entries
+// [beg, end) of row v: four consecutive entries at a time (16-byte loads),
+// the four neighbours' part and destination gathers in flight together
 template <class PT>
-__device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
-    const int lane = threadIdx.x & 31;
-    const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
-    const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
+__device__ __forceinline__ int32_t ab_sum(const ApplyArgs& A, int64_t beg, int64_t end, int t, int nt, int64_t v,
+                                          int32_t p, int32_t d, int32_t gv) {
     int32_t g2 = 0;
     const bool v4 = aligned16(A.g.ci) && aligned16(A.g.ew);
-    for (int64_t base = beg & ~(int64_t)3; base < end; base += 128) {
+    for (int64_t base = beg & ~(int64_t)3; base < end; base += 4 * (int64_t)nt) {
         int32_t uu[4], ww[4], pu[4], du[4];
-        const int64_t e4 = base + 4 * lane;
+        const int64_t e4 = base + 4 * t;
         ld4_row(A.g.ci, e4, beg, end, v4, -1, uu);
         if (A.g.ew) ld4_row(A.g.ew, e4, beg, end, v4, 0, ww);
         else {
@@ -659,7 +659,15 @@ __device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* 
             g2 += q == d ? ww[c] : (q == p ? -ww[c] : 0);
         }
     }
-    g2 = warp_sum(g2);
+    return g2;
+}
+
+// one candidate row of 33..heavy_deg entries per warp, 128 entries per sweep
+template <class PT>
+__device__ __forceinline__ void ab_warp(const ApplyArgs& A, int64_t v, int64_t* delta, int64_t& moves) {
+    const int lane = threadIdx.x & 31;
+    const int32_t d = A.dest[v], p = A.part[v], gv = A.gain[v];
+    const int32_t g2 = warp_sum(ab_sum<PT>(A, A.g.rp[v], A.g.rp[v + 1], lane, 32, v, p, d, gv));
     if (lane == 0 && g2 >= 0) ab_commit<PT>(A, v, p, d, delta, moves);
 }
 
@@ -678,9 +686,7 @@ __global__ void __launch_bounds__(RT) k_lp_apply(ApplyArgs A) {
         if (d >= 0) {
             const int nit = A.row_items[h];
             const int32_t p = A.part[v], gv = A.gain[v];
-            int32_t g2 = 0;
-            for (int64_t e = A.item_beg[blockIdx.x] + threadIdx.x; e < A.item_end[blockIdx.x]; e += RT)
-                g2 += ab_term<PT>(A.g, e, v, p, d, gv, A.pc, A.dest, A.gain);
+            int32_t g2 = ab_sum<PT>(A, A.item_beg[blockIdx.x], A.item_end[blockIdx.x], threadIdx.x, RT, v, p, d, gv);
             g2 = warp_sum(g2);
             if (lane == 0) s_red[w] = g2;
             __syncthreads();
