@@ -579,8 +579,11 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 //   A  d <= 128        one warp, 256-slot table in shared memory
 //   A2 d <= 256        one warp, 512-slot table
 //   B  d <= 512        one warp, 1024-slot table (11 KB per warp: 20 warps per SM)
-//   C  d <= 4096       one CTA of 512 threads, two-phase (first position kept by
-//                      atomicMax of deg - j), 8192-slot table on chip
+//   C1 d <= 2048       one CTA of 256 threads, two-phase (first position kept by
+//                      atomicMax of deg - j), 4096-slot table on chip (54 KB: four
+//                      CTAs per SM)
+//   C  d <= 4096       the same with 512 threads and an 8192-slot table (108 KB: two
+//                      CTAs per SM)
 //   C2 d <= 12288      the same with 1024 threads and a 16384-slot table (196 KB:
 //                      one CTA per SM; load factor at most 3/4)
 //   C3 d <= 65536      one 1024-thread CTA, the C2 table in P = 2..8 passes: pass p
@@ -594,6 +597,7 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 constexpr int TA_ROW = 128, TA_SLOTS = 256;
 constexpr int TA2_ROW = 256, TA2_SLOTS = 512;
 constexpr int TB_ROW = 512, TB_SLOTS = 1024, TB_WARPS = 4;
+constexpr int TC1_ROW = 2048, TC1_SLOTS = 4096, TC1_T = 256;
 constexpr int TC_ROW = 4096, TC_SLOTS = 8192, TC_T = 512;
 constexpr int TC2_ROW = 12288, TC2_SLOTS = 16384, TC2_T = 1024;
 constexpr int TC3_ROW = 65536, TC3_KEYS = 12288;   // at most TC3_KEYS walk entries per pass on average
@@ -747,17 +751,21 @@ __device__ __forceinline__ int32_t block_scan_excl(int32_t x, int32_t* sh, int32
     return r;
 }
 
-// rows longer than TB_ROW: lists of the on-chip tiers C (<= TC_ROW), C2
-// (<= TC2_ROW), C3 (<= TC3_ROW) and of tier D.  count[0] = rows of tier C,
-// count[1] = rows of tier D, count[2] = longest tier-D row, count[3] = rows of
-// tier C2, count[4] = rows of tier C3
-__global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC,
-                            int32_t* __restrict__ listC2, int32_t* __restrict__ listC3, int32_t* __restrict__ listD,
-                            int64_t* __restrict__ count) {
+// rows longer than TB_ROW: lists of the on-chip tiers C1 (<= TC1_ROW), C
+// (<= TC_ROW), C2 (<= TC2_ROW), C3 (<= TC3_ROW) and of tier D.  count[0] =
+// rows of tier C, count[1] = rows of tier D, count[2] = longest tier-D row,
+// count[3] = rows of tier C2, count[4] = rows of tier C3, count[5] = rows of
+// tier C1
+__global__ void k_long_rows(int64_t nc, const int64_t* __restrict__ cdeg, int32_t* __restrict__ listC1,
+                            int32_t* __restrict__ listC, int32_t* __restrict__ listC2, int32_t* __restrict__ listC3,
+                            int32_t* __restrict__ listD, int64_t* __restrict__ count) {
     for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = cdeg[c];
         if (d <= TB_ROW) continue;
-        if (d <= TC_ROW) {
+        if (d <= TC1_ROW) {
+            unsigned long long slot = atomicAdd((unsigned long long*)&count[5], 1ull);
+            listC1[slot] = (int32_t)c;
+        } else if (d <= TC_ROW) {
             unsigned long long slot = atomicAdd((unsigned long long*)&count[0], 1ull);
             listC[slot] = (int32_t)c;
         } else if (d <= TC2_ROW) {
@@ -1286,13 +1294,14 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     int32_t* tci = c.tmp_alloc<int32_t>(T);
     int32_t* tew = c.tmp_alloc<int32_t>(T);
     int32_t* rowcnt = c.tmp_alloc<int32_t>(nc);
+    int32_t* listC1 = c.tmp_alloc<int32_t>(nc);
     int32_t* listC = c.tmp_alloc<int32_t>(nc);
     int32_t* listC2 = c.tmp_alloc<int32_t>(nc);
     int32_t* listC3 = c.tmp_alloc<int32_t>(nc);
     int32_t* listD = c.tmp_alloc<int32_t>(nc);
-    int64_t* lcount = c.tmp_alloc<int64_t>(5);
+    int64_t* lcount = c.tmp_alloc<int64_t>(6);
     int32_t* err = c.tmp_alloc<int32_t>(1);
-    memset_async(c, lcount, 0, 5 * sizeof(int64_t));
+    memset_async(c, lcount, 0, 6 * sizeof(int64_t));
     memset_async(c, err, 0, sizeof(int32_t));
     {
         constexpr size_t smA = 8 * warp_dedup_smem<TA_ROW, TA_SLOTS, int32_t>();
@@ -1311,12 +1320,19 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
             g, fine.cmap, mem, nc, TA2_ROW + 1, off, cdeg, tci, tew, rowcnt);
         GP_LAUNCHED(c);
     }
-    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC, listC2, listC3, listD, lcount);
+    k_long_rows<<<grid_for(nc, 256), 256, 0, c.s>>>(nc, cdeg, listC1, listC, listC2, listC3, listD, lcount);
     GP_LAUNCHED(c);
-    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 5 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    GP_CUDA(cudaMemcpyAsync(c.h_pinned, lcount, 6 * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
     c.sync();
     const int64_t nC = c.h_pinned[0], nD = c.h_pinned[1], maxD = c.h_pinned[2], nC2 = c.h_pinned[3];
-    const int64_t nC3 = c.h_pinned[4];
+    const int64_t nC3 = c.h_pinned[4], nC1 = c.h_pinned[5];
+    if (nC1 > 0) {
+        k_dedup_cta_smem<TC1_T, TC1_SLOTS, TC1_ROW>
+            <<<(unsigned)std::min<int64_t>(nC1, (int64_t)c.sm_count * c.ctas_per_sm), TC1_T,
+               cta_dedup_smem<TC1_SLOTS, TC1_ROW>(), c.s>>>(g, fine.cmap, mem, listC1, nC1, off, cdeg, tci, tew, rowcnt,
+                                                            err);
+        GP_LAUNCHED(c);
+    }
     if (nC > 0) {
         // one CTA per row: the block scheduler balances rows of unequal length
         k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>
@@ -1438,6 +1454,8 @@ void coarsen_smem_caps() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA2));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_warp<TB_ROW, TB_SLOTS, TB_WARPS, int16_t>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB));
+    GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC1_T, TC1_SLOTS, TC1_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_dedup_smem<TC1_SLOTS, TC1_ROW>()));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC_T, TC_SLOTS, TC_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_dedup_smem<TC_SLOTS, TC_ROW>()));
     GP_CUDA(cudaFuncSetAttribute(k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
