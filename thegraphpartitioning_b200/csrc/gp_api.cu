@@ -86,21 +86,58 @@ __global__ void k_check_rowptr(int64_t n, int64_t m, const int64_t* __restrict__
     if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)&sums[0], (unsigned long long)local);
 }
 
-__global__ void k_check_rows(int64_t n, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+// one entry: weight >= 1, column id in range, no self loop (the smallest
+// (code, index) reported wins, whatever the order of the checks)
+__device__ __forceinline__ void check_entry(int64_t n, int64_t e, int64_t v, int32_t u, int32_t w, int check,
+                                            unsigned long long* err, int64_t& local) {
+    if (w < 1) report(err, V_EWGT, e);
+    local += w;
+    if (check >= 1) {
+        if (u < 0 || u >= n) report(err, V_COLIDX, e);
+        else if (u == v) report(err, V_SELF, v);
+    }
+}
+// entries of a row-pointer-checked CSR, entry-sliced (csr_row_of /
+// csr_window_lane), eight groups of 32 entries loaded together
+__global__ void k_check_rows(int64_t n, int64_t m, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
                              const int32_t* __restrict__ ew, int check, unsigned long long* err, int64_t* sums) {
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nslice = (m + CSR_SLICE - 1) / CSR_SLICE;
     int64_t local = 0;
-    for (int64_t v = wid; v < n; v += nw) {
-        for (int64_t e = rp[v] + lane; e < rp[v + 1]; e += 32) {
-            const int32_t w = ew ? ew[e] : 1;
-            if (w < 1) report(err, V_EWGT, e);
-            local += w;
-            if (check >= 1) {
-                const int32_t u = ci[e];
-                if (u < 0 || u >= n) report(err, V_COLIDX, e);
-                else if (u == v) report(err, V_SELF, v);
+    for (int64_t sl = wid; sl < nslice; sl += nw) {
+        const int64_t o0 = sl * CSR_SLICE, o1 = o0 + CSR_SLICE < m ? o0 + CSR_SLICE : m;
+        int64_t cb = csr_row_of(rp, n, o0), s = 0, wend = 0;
+        auto window = [&]() {
+            s = cb + lane < n ? rp[cb + lane] : m;
+            wend = rp[cb + 32 < n ? cb + 32 : n];
+        };
+        window();
+        int64_t o = o0;
+        while (o < o1) {
+            const int64_t lim = o1 < wend ? o1 : wend;
+            if (o + 256 <= lim) {
+                int32_t u[8], w[8];
+                int64_t v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int64_t oi = o + 32 * q + lane;
+                    v[q] = cb + csr_window_lane(s, oi);
+                    u[q] = check >= 1 ? __ldcs(&ci[oi]) : 0;
+                    w[q] = ew ? __ldcs(&ew[oi]) : 1;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) check_entry(n, o + 32 * q + lane, v[q], u[q], w[q], check, err, local);
+                o += 256;
+            } else if (o < lim) {
+                const int64_t oi = o + lane;
+                const int64_t v = cb + csr_window_lane(s, oi);
+                if (oi < lim) check_entry(n, oi, v, check >= 1 ? ci[oi] : 0, ew ? ew[oi] : 1, check, err, local);
+                o = o + 32 < lim ? o + 32 : lim;
+            } else {
+                cb += 32;   // o >= wend: o lies in a later row
+                window();
             }
         }
     }
@@ -174,7 +211,8 @@ static int64_t validate(Ctx& c, const DGraph& g, int check) {
     c.sync();
     uint64_t e0 = (uint64_t)c.h_pinned[0];
     if (e0 != ~0ull) throw GpError(GP_EINVAL, verr((int)(e0 >> 48), (int64_t)(e0 & ((1ull << 48) - 1))));
-    k_check_rows<<<grid_for(g.n * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(g.n, g.rp, g.ci, g.ew, check, err, sums);
+    k_check_rows<<<grid_for((g.m + CSR_SLICE - 1) / CSR_SLICE * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(
+        g.n, g.m, g.rp, g.ci, g.ew, check, err, sums);
     GP_LAUNCHED(c);
     c.bytes += 8 * (g.n + 1) + (g.vw ? 4 * g.n : 0) + (check >= 1 ? 4 * g.m : 0) + (g.ew ? 4 * g.m : 0);
     GP_CUDA(cudaMemcpyAsync(c.h_pinned, err, 8, cudaMemcpyDeviceToHost, c.s));

@@ -1207,14 +1207,9 @@ __global__ void k_td_rows(const int32_t* __restrict__ list, int64_t n, const int
 // 32 consecutive rows (start and source offset, one row per lane); the row of
 // an output position is the last window row starting at or before it (five
 // shuffle steps).  Eight groups of 32 entries are loaded before any is stored.
-constexpr int64_t CP_SLICE = 16384;
+constexpr int64_t CP_SLICE = CSR_SLICE;
 __device__ __forceinline__ int64_t cp_source(int64_t oi, int64_t s, int64_t src) {
-    int l = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-        const int64_t sv = __shfl_sync(0xffffffffu, s, l + step);
-        if (sv <= oi) l += step;
-    }
+    const int l = csr_window_lane(s, oi);
     return __shfl_sync(0xffffffffu, src, l) + (oi - __shfl_sync(0xffffffffu, s, l));
 }
 __global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, int64_t cm, const int64_t* __restrict__ off,
@@ -1227,12 +1222,7 @@ __global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, int64_t cm, c
     const int64_t nslice = (cm + CP_SLICE - 1) / CP_SLICE;
     for (int64_t sl = wid; sl < nslice; sl += nw) {
         const int64_t o0 = sl * CP_SLICE, o1 = o0 + CP_SLICE < cm ? o0 + CP_SLICE : cm;
-        int64_t lo = 0, hi = nc - 1;   // last row with crp[row] <= o0
-        while (lo < hi) {
-            const int64_t mid = (lo + hi + 1) >> 1;
-            if (crp[mid] <= o0) lo = mid; else hi = mid - 1;
-        }
-        int64_t cb = lo, s = 0, src = 0, wend = 0;
+        int64_t cb = csr_row_of(crp, nc, o0), s = 0, src = 0, wend = 0;
         auto window = [&]() {   // rows cb .. cb + 31; wend = first output entry past them
             const int64_t r = cb + lane;
             s = r < nc ? crp[r] : cm;

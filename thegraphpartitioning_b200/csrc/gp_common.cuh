@@ -141,6 +141,29 @@ __device__ __forceinline__ void group_argmax64(uint32_t mask, uint64_t& k, int32
     k = ((uint64_t)mh << 32) | ml;
     id = (int32_t)mi;
 }
+// Entry slices of a CSR (rp: n + 1 row starts, nondecreasing): the row holding
+// entry o is the last row starting at or before it (empty rows share starts).
+// A warp walking a slice of entries keeps a window of 32 consecutive rows, one
+// start per lane (rows past n start at m); csr_window_lane gives the lane of
+// the window row holding entry oi, which must lie inside the window.
+__device__ __forceinline__ int64_t csr_row_of(const int64_t* __restrict__ rp, int64_t n, int64_t o) {
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (rp[mid] <= o) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+__device__ __forceinline__ int csr_window_lane(int64_t s, int64_t oi) {
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+        const int64_t sv = __shfl_sync(0xffffffffu, s, l + step);
+        if (sv <= oi) l += step;
+    }
+    return l;
+}
+constexpr int64_t CSR_SLICE = 16384;   // entries per warp of an entry-sliced pass
 // The same argmax and a sum over aligned groups of TILE lanes (TILE a power of
 // two <= 32; every lane of the warp calls them).  A group smaller than the
 // warp reduces with butterfly shuffles inside the group: a redux.sync whose

@@ -878,16 +878,57 @@ __global__ void k_part_weights(int64_t n, const int32_t* __restrict__ part, cons
 }
 
 // warp per row: directed cross weight (d_cross2 accumulates 2*cut)
+// directed cross weight, entry-sliced (csr_row_of / csr_window_lane): each
+// lane of a window also holds its row's part; eight groups of 32 entries have
+// their column ids loaded, then their neighbours' parts gathered, together
 __global__ void __launch_bounds__(RT) k_cut(DGraph g, const int32_t* __restrict__ part, int64_t* __restrict__ cross2) {
     __shared__ int64_t s_red[RW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t wid = ((int64_t)blockIdx.x * RT + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * RT) >> 5;
+    const int64_t n = g.n, m = g.m, nslice = (m + CSR_SLICE - 1) / CSR_SLICE;
     int64_t acc = 0;
-    for (int64_t v = wid; v < g.n; v += nw) {
-        const int32_t p = part[v];
-        for (int64_t e = g.rp[v] + lane; e < g.rp[v + 1]; e += 32)
-            if (part[__ldcs(&g.ci[e])] != p) acc += g.ew ? __ldcs(&g.ew[e]) : 1;
+    for (int64_t sl = wid; sl < nslice; sl += nw) {
+        const int64_t o0 = sl * CSR_SLICE, o1 = o0 + CSR_SLICE < m ? o0 + CSR_SLICE : m;
+        int64_t cb = csr_row_of(g.rp, n, o0), s = 0, wend = 0;
+        int32_t pv = 0;
+        auto window = [&]() {
+            const int64_t r = cb + lane;
+            s = r < n ? g.rp[r] : m;
+            pv = r < n ? part[r] : 0;
+            wend = g.rp[cb + 32 < n ? cb + 32 : n];
+        };
+        window();
+        int64_t o = o0;
+        while (o < o1) {
+            const int64_t lim = o1 < wend ? o1 : wend;
+            if (o + 256 <= lim) {
+                int32_t u[8], pr[8], wt[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int64_t oi = o + 32 * q + lane;
+                    pr[q] = __shfl_sync(0xffffffffu, pv, csr_window_lane(s, oi));
+                    u[q] = __ldcs(&g.ci[oi]);
+                    wt[q] = g.ew ? __ldcs(&g.ew[oi]) : 1;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) u[q] = GP_IN(u[q], n) ? part[u[q]] : pr[q];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc += u[q] != pr[q] ? wt[q] : 0;
+                o += 256;
+            } else if (o < lim) {
+                const int64_t oi = o + lane;
+                const int32_t p = __shfl_sync(0xffffffffu, pv, csr_window_lane(s, oi));
+                if (oi < lim) {
+                    const int32_t u = __ldcs(&g.ci[oi]);
+                    if (GP_IN(u, n) && part[u] != p) acc += g.ew ? __ldcs(&g.ew[oi]) : 1;
+                }
+                o = o + 32 < lim ? o + 32 : lim;
+            } else {
+                cb += 32;   // o >= wend: o lies in a later row
+                window();
+            }
+        }
     }
     acc = warp_sum(acc);
     if (lane == 0) s_red[w] = acc;
@@ -914,7 +955,8 @@ void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64
 
 void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw) {
     memset_async(c, d_cross2, 0, sizeof(int64_t));
-    k_cut<<<grid_for(g.n * 32, RT, c.sm_count * c.ctas_per_sm), RT, 0, c.s>>>(g, part, d_cross2);
+    k_cut<<<grid_for((g.m + CSR_SLICE - 1) / CSR_SLICE * 32, RT, c.sm_count * c.ctas_per_sm), RT, 0, c.s>>>(g, part,
+                                                                                                       d_cross2);
     GP_LAUNCHED(c);
     c.bytes += 8 * (g.n + 1) + 8 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.n;
     if (d_pw) part_weights(c, g, part, k, d_pw);
