@@ -99,15 +99,16 @@ __device__ __forceinline__ void check_entry(int64_t n, int64_t e, int64_t v, int
 }
 // entries of a row-pointer-checked CSR, entry-sliced (csr_row_of /
 // csr_window_lane), eight groups of 32 entries loaded together
-__global__ void k_check_rows(int64_t n, int64_t m, const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+__global__ void k_check_rows(int64_t n, int64_t m, int64_t slice, const int64_t* __restrict__ rp,
+                             const int32_t* __restrict__ ci,
                              const int32_t* __restrict__ ew, int check, unsigned long long* err, int64_t* sums) {
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t nslice = (m + CSR_SLICE - 1) / CSR_SLICE;
+    const int64_t nslice = (m + slice - 1) / slice;
     int64_t local = 0;
     for (int64_t sl = wid; sl < nslice; sl += nw) {
-        const int64_t o0 = sl * CSR_SLICE, o1 = o0 + CSR_SLICE < m ? o0 + CSR_SLICE : m;
+        const int64_t o0 = sl * slice, o1 = o0 + slice < m ? o0 + slice : m;
         int64_t cb = csr_row_of(rp, n, o0), s = 0, wend = 0;
         auto window = [&]() {
             s = cb + lane < n ? rp[cb + lane] : m;
@@ -211,8 +212,9 @@ static int64_t validate(Ctx& c, const DGraph& g, int check) {
     c.sync();
     uint64_t e0 = (uint64_t)c.h_pinned[0];
     if (e0 != ~0ull) throw GpError(GP_EINVAL, verr((int)(e0 >> 48), (int64_t)(e0 & ((1ull << 48) - 1))));
-    k_check_rows<<<grid_for((g.m + CSR_SLICE - 1) / CSR_SLICE * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(
-        g.n, g.m, g.rp, g.ci, g.ew, check, err, sums);
+    const int64_t slice = csr_slice(g.m, c.sm_count);
+    k_check_rows<<<grid_for((g.m + slice - 1) / slice * 32, 256, c.sm_count * 8), 256, 0, c.s>>>(
+        g.n, g.m, slice, g.rp, g.ci, g.ew, check, err, sums);
     GP_LAUNCHED(c);
     c.bytes += 8 * (g.n + 1) + (g.vw ? 4 * g.n : 0) + (check >= 1 ? 4 * g.m : 0) + (g.ew ? 4 * g.m : 0);
     GP_CUDA(cudaMemcpyAsync(c.h_pinned, err, 8, cudaMemcpyDeviceToHost, c.s));

@@ -1202,26 +1202,26 @@ __global__ void k_td_rows(const int32_t* __restrict__ list, int64_t n, const int
 // warp per coarse row: temporary (walk-bound offsets) -> final CSR
 // Packs every row's deduplicated entries (crp[c + 1] - crp[c] of them at
 // walk offset off[c] of tci / tew) into the coarse CSR.  The output is cut
-// into slices of CP_SLICE entries, one warp each: the warp finds the row
+// into slices of `slice` entries (csr_slice), one warp each: the warp finds the row
 // holding its first entry by binary search over crp, then keeps a window of
 // 32 consecutive rows (start and source offset, one row per lane); the row of
 // an output position is the last window row starting at or before it (five
 // shuffle steps).  Eight groups of 32 entries are loaded before any is stored.
-constexpr int64_t CP_SLICE = CSR_SLICE;
 __device__ __forceinline__ int64_t cp_source(int64_t oi, int64_t s, int64_t src) {
     const int l = csr_window_lane(s, oi);
     return __shfl_sync(0xffffffffu, src, l) + (oi - __shfl_sync(0xffffffffu, s, l));
 }
-__global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, int64_t cm, const int64_t* __restrict__ off,
+__global__ void __launch_bounds__(256) k_contract_copy(int64_t nc, int64_t cm, int64_t slice,
+                                                       const int64_t* __restrict__ off,
                                                        const int64_t* __restrict__ crp, const int32_t* __restrict__ tci,
                                                        const int32_t* __restrict__ tew, int32_t* __restrict__ ci,
                                                        int32_t* __restrict__ ew) {
     const int lane = threadIdx.x & 31;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t nslice = (cm + CP_SLICE - 1) / CP_SLICE;
+    const int64_t nslice = (cm + slice - 1) / slice;
     for (int64_t sl = wid; sl < nslice; sl += nw) {
-        const int64_t o0 = sl * CP_SLICE, o1 = o0 + CP_SLICE < cm ? o0 + CP_SLICE : cm;
+        const int64_t o0 = sl * slice, o1 = o0 + slice < cm ? o0 + slice : cm;
         int64_t cb = csr_row_of(crp, nc, o0), s = 0, src = 0, wend = 0;
         auto window = [&]() {   // rows cb .. cb + 31; wend = first output entry past them
             const int64_t r = cb + lane;
@@ -1417,8 +1417,9 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
     if ((int32_t)c.h_pinned[1] != 0) throw GpError(GP_EINTERNAL, "contraction hash table overflow");
     int32_t* cci = c.keep_alloc<int32_t>(mc);
     int32_t* cew = c.keep_alloc<int32_t>(mc);
-    k_contract_copy<<<grid_for((mc + CP_SLICE - 1) / CP_SLICE * 32, 256, c.sm_count * c.ctas_per_sm), 256, 0, c.s>>>(
-        nc, mc, off, crp, tci, tew, cci, cew);
+    const int64_t cslice = csr_slice(mc, c.sm_count);
+    k_contract_copy<<<grid_for((mc + cslice - 1) / cslice * 32, 256, c.sm_count * c.ctas_per_sm), 256, 0, c.s>>>(
+        nc, mc, cslice, off, crp, tci, tew, cci, cew);
     GP_LAUNCHED(c);
     // rows read twice (count and rank for long rows), cmap gathered per entry,
     // unique entries written to the temporary and copied once

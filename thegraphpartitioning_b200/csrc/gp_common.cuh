@@ -163,7 +163,13 @@ __device__ __forceinline__ int csr_window_lane(int64_t s, int64_t oi) {
     }
     return l;
 }
-constexpr int64_t CSR_SLICE = 16384;   // entries per warp of an entry-sliced pass
+// entries per warp of an entry-sliced pass over m entries: about 32 warps
+// per SM, at least 256 and at most 16384 entries each (a multiple of 256)
+inline int64_t csr_slice(int64_t m, int sm_count) {
+    int64_t s = (m + (int64_t)sm_count * 32 - 1) / ((int64_t)sm_count * 32);
+    s = (s + 255) & ~(int64_t)255;
+    return s < 256 ? 256 : (s > 16384 ? 16384 : s);
+}
 // The same argmax and a sum over aligned groups of TILE lanes (TILE a power of
 // two <= 32; every lane of the warp calls them).  A group smaller than the
 // warp reduces with butterfly shuffles inside the group: a redux.sync whose

@@ -881,15 +881,16 @@ __global__ void k_part_weights(int64_t n, const int32_t* __restrict__ part, cons
 // directed cross weight, entry-sliced (csr_row_of / csr_window_lane): each
 // lane of a window also holds its row's part; eight groups of 32 entries have
 // their column ids loaded, then their neighbours' parts gathered, together
-__global__ void __launch_bounds__(RT) k_cut(DGraph g, const int32_t* __restrict__ part, int64_t* __restrict__ cross2) {
+__global__ void __launch_bounds__(RT) k_cut(DGraph g, int64_t slice, const int32_t* __restrict__ part,
+                                            int64_t* __restrict__ cross2) {
     __shared__ int64_t s_red[RW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t wid = ((int64_t)blockIdx.x * RT + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * RT) >> 5;
-    const int64_t n = g.n, m = g.m, nslice = (m + CSR_SLICE - 1) / CSR_SLICE;
+    const int64_t n = g.n, m = g.m, nslice = (m + slice - 1) / slice;
     int64_t acc = 0;
     for (int64_t sl = wid; sl < nslice; sl += nw) {
-        const int64_t o0 = sl * CSR_SLICE, o1 = o0 + CSR_SLICE < m ? o0 + CSR_SLICE : m;
+        const int64_t o0 = sl * slice, o1 = o0 + slice < m ? o0 + slice : m;
         int64_t cb = csr_row_of(g.rp, n, o0), s = 0, wend = 0;
         int32_t pv = 0;
         auto window = [&]() {
@@ -955,8 +956,9 @@ void part_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64
 
 void cut_and_weights(Ctx& c, const DGraph& g, const int32_t* part, int32_t k, int64_t* d_cross2, int64_t* d_pw) {
     memset_async(c, d_cross2, 0, sizeof(int64_t));
-    k_cut<<<grid_for((g.m + CSR_SLICE - 1) / CSR_SLICE * 32, RT, c.sm_count * c.ctas_per_sm), RT, 0, c.s>>>(g, part,
-                                                                                                       d_cross2);
+    const int64_t slice = csr_slice(g.m, c.sm_count);
+    k_cut<<<grid_for((g.m + slice - 1) / slice * 32, RT, c.sm_count * c.ctas_per_sm), RT, 0, c.s>>>(g, slice, part,
+                                                                                                   d_cross2);
     GP_LAUNCHED(c);
     c.bytes += 8 * (g.n + 1) + 8 * g.m + (g.ew ? 4 * g.m : 0) + 4 * g.n;
     if (d_pw) part_weights(c, g, part, k, d_pw);
