@@ -357,6 +357,7 @@ void vc_begin(Ctx& c, const DGraph& g0, int32_t k, float imbalance, uint64_t see
     B.pc = c.keep_alloc<uint16_t>(n0);
     B.pc_next = c.keep_alloc<uint16_t>(n0);
     B.dest = c.keep_alloc<int32_t>(n0);
+    B.pdg = k <= 1024 ? c.keep_alloc<uint64_t>(n0) : nullptr;
     B.gain = c.keep_alloc<int32_t>(n0);
     B.mp = P.gnn && gnn_has_move_head(P.gnn) ? c.keep_alloc<int32_t>(n0) : nullptr;
     B.lock = c.keep_alloc<uint8_t>(n0);

@@ -104,6 +104,8 @@ struct RefineBufs {
     int32_t* dest = nullptr;
     int32_t* gain = nullptr;
     int32_t* mp = nullptr;        // learned move priorities of a label-propagation step
+    uint64_t* pdg = nullptr;      // label-propagation passes, k <= 1024: part, dest + 1 and gain of
+                                  // every vertex in one word (the move step's one gather per entry)
     uint8_t* lock = nullptr;
     uint8_t* lock_next = nullptr;
     int64_t* pw = nullptr;        // k

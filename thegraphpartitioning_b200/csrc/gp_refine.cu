@@ -123,7 +123,17 @@ struct ConnArgs {
     int32_t* hhist;
     int64_t* hsum;
     int32_t* hdone;
+    uint64_t* pdg;              // label propagation: pdg_pack(part, dest, gain) per row (nullptr: none)
 };
+
+// one word per vertex for the move step: part (bits 44-53), dest + 1 (bits
+// 32-43; 0: no proposal) and gain (bits 0-31); k <= 1024
+__device__ __forceinline__ uint64_t pdg_pack(int32_t p, int32_t d, int32_t g) {
+    return ((uint64_t)(uint32_t)p << 44) | ((uint64_t)(uint32_t)(d + 1) << 32) | (uint64_t)(uint32_t)g;
+}
+__device__ __forceinline__ int32_t pdg_part(uint64_t x) { return (int32_t)((x >> 44) & 0x3FFu); }
+__device__ __forceinline__ int32_t pdg_dest(uint64_t x) { return (int32_t)((x >> 32) & 0xFFFu) - 1; }
+__device__ __forceinline__ int32_t pdg_gain(uint64_t x) { return (int32_t)(uint32_t)x; }
 
 // part id of neighbour u from the gather copy (read-only in the kernel)
 template <class PT>
@@ -178,6 +188,7 @@ __device__ __forceinline__ bool conn_decide(const ConnArgs& A, int mode, bool ac
     }
     A.dest[v] = d;
     A.gain[v] = gn;
+    if (mode == MODE_LP && A.pdg) A.pdg[v] = pdg_pack(p, d, gn);
     return cand;
 }
 
@@ -559,15 +570,19 @@ __global__ void __launch_bounds__(RT, 5) k_conn(ConnArgs A) {
 template <class PT>
 __device__ __forceinline__ int32_t ab_term(const DGraph& g, int64_t e, int64_t v, int32_t p, int32_t d, int32_t gv,
                                            const void* pc, const int32_t* __restrict__ dest,
-                                           const int32_t* __restrict__ gain) {
+                                           const int32_t* __restrict__ gain, const uint64_t* __restrict__ pdg) {
     const int32_t u = __ldcs(&g.ci[e]);
     if (!GP_IN(u, g.n)) return 0;
-    int32_t pu = gpart<PT>(pc, u, g.n);
-    const int32_t du = dest[u];
-    if (du >= 0) {
-        const int32_t gu = gain[u];
-        if (gu > gv || (gu == gv && u < (int32_t)v)) pu = du;
+    int32_t pu, du, gu = 0;
+    if (pdg) {
+        const uint64_t x = pdg[u];
+        pu = pdg_part(x); du = pdg_dest(x); gu = pdg_gain(x);
+    } else {
+        pu = gpart<PT>(pc, u, g.n);
+        du = dest[u];
+        if (du >= 0) gu = gain[u];
     }
+    if (du >= 0 && (gu > gv || (gu == gv && u < (int32_t)v))) pu = du;
     const int32_t wt = g.ew ? __ldcs(&g.ew[e]) : 1;
     return pu == d ? wt : (pu == p ? -wt : 0);
 }
@@ -594,6 +609,7 @@ struct ApplyArgs {
     int64_t* moves_out;
     int64_t* hsum;
     int32_t* hdone;
+    const uint64_t* pdg;        // packed part / dest / gain of every vertex (nullptr: gather them apart)
 };
 
 template <class PT>
@@ -618,7 +634,7 @@ __device__ __forceinline__ void ab_tile(const ApplyArgs& A, int64_t v, int64_t* 
         d = A.dest[v]; p = A.part[v];
         const int32_t gv = A.gain[v];
         const int64_t e = A.g.rp[v] + tl;
-        if (e < A.g.rp[v + 1]) t = ab_term<PT>(A.g, e, v, p, d, gv, A.pc, A.dest, A.gain);
+        if (e < A.g.rp[v + 1]) t = ab_term<PT>(A.g, e, v, p, d, gv, A.pc, A.dest, A.gain, A.pdg);
     }
 #pragma unroll
     for (int o = TILE / 2; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
@@ -642,20 +658,29 @@ __device__ __forceinline__ int32_t ab_sum(const ApplyArgs& A, int64_t beg, int64
 #pragma unroll
             for (int c = 0; c < 4; ++c) ww[c] = uu[c] >= 0 ? 1 : 0;
         }
+        int32_t gu[4];
+        if (A.pdg) {   // one gather per entry: part, dest and gain in one word
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const bool ok = uu[c] >= 0 && GP_IN(uu[c], A.g.n);
-            pu[c] = ok ? gpart<PT>(A.pc, uu[c], A.g.n) : -1;
-            du[c] = ok ? A.dest[uu[c]] : -1;
+            for (int c = 0; c < 4; ++c) {
+                const bool ok = uu[c] >= 0 && GP_IN(uu[c], A.g.n);
+                const uint64_t x = ok ? A.pdg[uu[c]] : 0ull;
+                pu[c] = ok ? pdg_part(x) : -1; du[c] = pdg_dest(x); gu[c] = pdg_gain(x);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const bool ok = uu[c] >= 0 && GP_IN(uu[c], A.g.n);
+                pu[c] = ok ? gpart<PT>(A.pc, uu[c], A.g.n) : -1;
+                du[c] = ok ? A.dest[uu[c]] : -1;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) gu[c] = du[c] >= 0 ? A.gain[uu[c]] : 0;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             if (uu[c] < 0 || pu[c] < 0) continue;
             int32_t q = pu[c];
-            if (du[c] >= 0) {
-                const int32_t gu = A.gain[uu[c]];
-                if (gu > gv || (gu == gv && uu[c] < (int32_t)v)) q = du[c];
-            }
+            if (du[c] >= 0 && (gu[c] > gv || (gu[c] == gv && uu[c] < (int32_t)v))) q = du[c];
             g2 += q == d ? ww[c] : (q == p ? -ww[c] : 0);
         }
     }
@@ -1281,7 +1306,7 @@ __device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
         CA.wfirst = nullptr;
         CA.dest = R.dest; CA.gain = R.gain; CA.status = R.status;
         CA.part_next = nullptr; CA.lock_next = nullptr;
-        CA.pc = part; CA.pc_next = nullptr;
+        CA.pc = part; CA.pc_next = nullptr; CA.pdg = nullptr;
         CA.hhist = nullptr; CA.hsum = nullptr; CA.hdone = nullptr;
         int64_t acc = 0;
         int32_t* hist = s_hist + w * k;
@@ -1342,7 +1367,7 @@ __device__ void cta_refine_level(const CtaRefineArgs& R, unsigned char* rsm) {
             for (int b = 0; b < 3; ++b) AA.clist[b] = R.clist[b];
             AA.status = R.status; AA.part_next = part_next; AA.lock_next = lock_next; AA.pw = nullptr;
             AA.pc = part; AA.pc_next = nullptr;
-            AA.moves_out = nullptr; AA.hsum = nullptr; AA.hdone = nullptr;
+            AA.moves_out = nullptr; AA.hsum = nullptr; AA.hdone = nullptr; AA.pdg = nullptr;
             for (int64_t u = w; u < U2 + U1 + U0; u += CW) {
                 if (u < U2) {
                     const int64_t v = R.bucket[2][u];
@@ -1685,7 +1710,7 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
         CA.wfirst = B.wfirst;
         CA.dest = B.dest; CA.gain = B.gain; CA.status = B.status;
         CA.part_next = B.part_next; CA.lock_next = B.lock_next;   // the LP step's starting copy
-        CA.pc = B.pc; CA.pc_next = B.pc_next;
+        CA.pc = B.pc; CA.pc_next = B.pc_next; CA.pdg = B.pdg;
         if (B.pcb == 1) k_conn<uint8_t><<<grid, RT, conn_smem, c.s>>>(CA);
         else k_conn<uint16_t><<<grid, RT, conn_smem, c.s>>>(CA);
         GP_LAUNCHED(c);
@@ -1749,11 +1774,12 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
             for (int b = 0; b < 3; ++b) AA.clist[b] = B.clist[b];
             AA.status = B.status; AA.part_next = B.part_next; AA.lock_next = B.lock_next; AA.pw = B.pw;
             AA.moves_out = moves_d;
-            AA.pc = B.pc; AA.pc_next = B.pc_next;
+            AA.pc = B.pc; AA.pc_next = B.pc_next; AA.pdg = B.pdg;
             if (B.mp && P.gnn && gnn_has_move_head(P.gnn)) {
                 // learned order of the afterburner: (move priority, id) instead of (gain, id)
                 gnn_move_priorities(c, P.gnn, g, level, B.dest, B.gain, B.mp);
                 AA.gain = B.mp;
+                AA.pdg = nullptr;   // the packed words hold the gains
                 if (tr.on()) {
                     std::vector<int32_t> hm((size_t)n);
                     GP_CUDA(cudaMemcpyAsync(hm.data(), B.mp, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c.s));
