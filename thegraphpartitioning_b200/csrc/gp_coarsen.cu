@@ -143,6 +143,22 @@ __device__ __forceinline__ void argmax_merge(uint64_t& k, int32_t& id, uint64_t 
     if (k2 > k || (k2 == k && (uint32_t)i2 < (uint32_t)id)) { k = k2; id = i2; }
 }
 __device__ __forceinline__ void warp_argmax(uint64_t& k, int32_t& id) { group_argmax64(0xffffffffu, k, id); }
+// the two best distinct neighbours (by argmax_merge's order; a neighbour
+// listed twice counts with its larger key) among those offered so far
+__device__ __forceinline__ bool key_before(uint64_t k2, int32_t i2, uint64_t k, int32_t i) {
+    return k2 > k || (k2 == k && (uint32_t)i2 < (uint32_t)i);
+}
+__device__ __forceinline__ void top2_insert(uint64_t& k1, int32_t& i1, uint64_t& k2, int32_t& i2, uint64_t k,
+                                            int32_t i) {
+    if (i == i1) { if (k > k1) k1 = k; return; }
+    if (i == i2) {
+        if (k > k2) k2 = k;
+        if (key_before(k2, i2, k1, i1)) { const uint64_t tk = k1; const int32_t ti = i1; k1 = k2; i1 = i2; k2 = tk; i2 = ti; }
+        return;
+    }
+    if (key_before(k, i, k1, i1)) { k2 = k1; i2 = i1; k1 = k; i1 = i; }
+    else if (key_before(k, i, k2, i2)) { k2 = k; i2 = i; }
+}
 // block-wide; result valid in thread 0
 __device__ __forceinline__ void block_argmax(uint64_t& k, int32_t& id, uint64_t* sk, int32_t* sid) {
     warp_argmax(k, id);
@@ -186,6 +202,9 @@ struct MatchArgs {
     int64_t* nkeys;
     int nbits;
     const int32_t* prio;      // learned priorities per entry (nullptr: edge weights)
+    int2* cand;               // MODE 0, rows of 33+ entries (one piece): the two best eligible
+    uint8_t* cmore;           // neighbours of the row's last scan and whether it had more
+                              // (nullptr: no cache)
     const uint8_t* hdead;     // MODE 0: heavy rows left without an eligible neighbour (nullptr: none)
     int any_matched;          // MODE 0: 0 in the first round (no neighbour to look up in match[])
     int check_vw;             // MODE 0: 0 when no two vertices of the level can exceed maxvw
@@ -261,8 +280,21 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
         const int32_t h = A.item_row[blockIdx.x];
         const int64_t v = A.heavy[h];
         if (A.match[v] != -1 || (A.hdead && A.hdead[h])) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
+        const int nit = A.row_items[h];
+        // a row in one piece keeps its two best eligible neighbours (as the warp rows do)
+        const bool cached = MODE == 0 && A.cand && nit == 1;
+        if (cached && A.any_matched) {
+            const int2 cc = A.cand[v];
+            const int32_t m1 = cc.x >= 0 ? A.match[cc.x] : 0, m2 = cc.y >= 0 ? A.match[cc.y] : 0;
+            int32_t r = -2;
+            if (cc.x >= 0 && m1 == -1) r = cc.x;
+            else if (cc.y >= 0 && m2 == -1) r = cc.y;
+            else if (!A.cmore[v]) r = -1;
+            if (r != -2) { if (threadIdx.x == 0) A.out[v] = r; return; }
+        }
         const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
         uint64_t bk = 0; int32_t bid = -1;
+        uint64_t k2 = 0; int32_t i2 = -1, cnt = 0;
         const int64_t beg = A.item_beg[blockIdx.x], end = A.item_end[blockIdx.x];
         const int32_t* kw = A.prio ? A.prio : A.g.ew;
         const bool v4 = aligned16(A.g.ci) && aligned16(kw);
@@ -274,11 +306,32 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 if (uu[c] < 0 || !match_ok<MODE>(A, v, uu[c], vwv)) continue;
-                argmax_merge(bk, bid, edge_key(kw ? ww[c] : 1, edge_hash(A.salt, (int32_t)v, uu[c])), uu[c]);
+                const uint64_t key = edge_key(kw ? ww[c] : 1, edge_hash(A.salt, (int32_t)v, uu[c]));
+                if (cached) { top2_insert(bk, bid, k2, i2, key, uu[c]); ++cnt; }
+                else argmax_merge(bk, bid, key, uu[c]);
             }
         }
+        if (cached) {
+            __shared__ int32_t s_best, s_cnt;
+            const uint64_t k1 = bk;
+            const int32_t i1 = bid;
+            block_argmax(bk, bid, sk, sid);
+            if (threadIdx.x == 0) { s_best = bid; s_cnt = 0; }
+            __syncthreads();
+            uint64_t ks = i1 == s_best ? k2 : k1;
+            int32_t is = i1 == s_best ? i2 : i1;
+            block_argmax(ks, is, sk, sid);
+            const int32_t wc = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)cnt);
+            if (lane == 0 && wc) atomicAdd(&s_cnt, wc);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                A.cand[v] = make_int2(s_best, ks ? is : -1);
+                A.cmore[v] = s_cnt > 2 ? 1 : 0;
+                A.out[v] = s_best;
+            }
+            return;
+        }
         block_argmax(bk, bid, sk, sid);
-        const int nit = A.row_items[h];
         __shared__ int s_last;
         if (threadIdx.x == 0) {
             s_last = 1;
@@ -314,7 +367,19 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
             const int64_t v = A.list[2][u - U0 - U1];
             const bool valid = A.match[v] == -1;
             uint64_t bk = 0; int32_t bid = -1;
-            if (valid) {
+            bool scan = valid;
+            if (MODE == 0 && valid && A.cand && A.any_matched) {
+                // neighbours only ever become matched, so the best of the row's
+                // last two cached candidates that is still unmatched is its
+                // best eligible neighbour; with both matched and no third, none
+                const int2 cc = A.cand[v];
+                const int32_t m1 = cc.x >= 0 ? A.match[cc.x] : 0, m2 = cc.y >= 0 ? A.match[cc.y] : 0;
+                if (cc.x >= 0 && m1 == -1) { bid = cc.x; scan = false; }
+                else if (cc.y >= 0 && m2 == -1) { bid = cc.y; scan = false; }
+                else if (!A.cmore[v]) { bid = -1; scan = false; }
+            }
+            uint64_t k2 = 0; int32_t i2 = -1, cnt = 0;
+            if (scan) {
                 const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
                 const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
                 // 128 entries per sweep, four consecutive ones per lane (16-byte loads)
@@ -341,11 +406,26 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
                         const int32_t x = uu[c];
                         if (x < 0 || x == (int32_t)v) continue;
                         if (MODE == 0 && (mm[c] != -1 || (A.check_vw && vwv + vv[c] > A.maxvw))) continue;
-                        argmax_merge(bk, bid, edge_key(ww[c], edge_hash(A.salt, (int32_t)v, x)), x);
+                        const uint64_t key = edge_key(ww[c], edge_hash(A.salt, (int32_t)v, x));
+                        if (MODE == 0 && A.cand) { top2_insert(bk, bid, k2, i2, key, x); ++cnt; }
+                        else argmax_merge(bk, bid, key, x);
+                    }
+                }
+                const uint64_t k1 = bk;
+                const int32_t i1 = bid;
+                warp_argmax(bk, bid);
+                if (MODE == 0 && A.cand) {
+                    // second: each lane offers its best neighbour other than the row's best
+                    uint64_t sk = i1 == bid ? k2 : k1;
+                    int32_t si = i1 == bid ? i2 : i1;
+                    warp_argmax(sk, si);
+                    const int32_t tot = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)cnt);
+                    if (lane == 0) {
+                        A.cand[v] = make_int2(bid, sk ? si : -1);
+                        A.cmore[v] = tot > 2 ? 1 : 0;
                     }
                 }
             }
-            warp_argmax(bk, bid);
             if (MODE == 0) { if (lane == 0) A.out[v] = valid ? bid : -1; }
             else match_emit<MODE>(A, lane == 0 && valid, v, bid);
         }
@@ -458,6 +538,9 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     A.hdone = c.tmp_alloc<int32_t>(std::max<int64_t>(L.nheavy, 1));
     memset_async(c, A.hdone, 0, sizeof(int32_t) * std::max<int64_t>(L.nheavy, 1));
     A.maxvw = P.maxvw; A.keys = nullptr; A.nkeys = nullptr; A.nbits = 0; A.prio = prio;
+    // rows of 33+ entries keep their two best eligible neighbours between rounds (written by round 0)
+    A.cand = c.tmp_alloc<int2>(g.n);
+    A.cmore = c.tmp_alloc<uint8_t>(g.n);
     // weight cap: skip the per-neighbour weight check when the two heaviest
     // vertices of the level together stay within maxvw
     A.check_vw = 0;
@@ -511,6 +594,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         memset_async(c, d_cnt, 0, 2 * sizeof(int64_t));
         MatchArgs B2 = A;
         B2.hdead = nullptr;   // anchors: the top neighbour over all neighbours
+        B2.cand = nullptr; B2.cmore = nullptr;
         B2.any_matched = 1;
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
