@@ -791,12 +791,20 @@ __device__ __forceinline__ int64_t seg_start(const uint64_t* keys, int64_t i, ui
     return lo;
 }
 
+// first index of every key segment (key >> RB_SHIFT = d, d = 0..k) of a
+// sorted candidate list: k + 1 searches instead of one per candidate
+__global__ void k_seg_first(int64_t cnt, const uint64_t* __restrict__ keys, int32_t k, int64_t* __restrict__ first) {
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d <= k; d += (int64_t)gridDim.x * blockDim.x)
+        first[d] = seg_start(keys, cnt, (uint64_t)d);
+}
+
 // flag[i] = 1 when the move keeps its source within the excess prefix
-__global__ void k_rb_source(int64_t cnt, const uint64_t* __restrict__ keys, const int64_t* __restrict__ pre,
-                            const int64_t* __restrict__ pw, int64_t Lmax, int32_t* __restrict__ flag) {
+__global__ void k_rb_source(int64_t cnt, const uint64_t* __restrict__ keys, const int64_t* __restrict__ segf,
+                            const int64_t* __restrict__ pre, const int64_t* __restrict__ pw, int64_t Lmax,
+                            int32_t* __restrict__ flag) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t src = keys[i] >> RB_SHIFT;
-        const int64_t s = seg_start(keys, i, src);
+        const int64_t s = segf[src];
         flag[i] = (pre[i] - pre[s]) < (pw[src] - Lmax) ? 1 : 0;
     }
 }
@@ -814,26 +822,47 @@ __global__ void k_rb_rekey(int64_t cnt, const uint64_t* __restrict__ keys, const
     }
 }
 
+// part-weight changes and moves of a block, added to the global totals once
+// per part (dynamic shared memory: k int64)
+__device__ __forceinline__ void rb_delta_begin(int64_t* delta, int32_t k) {
+    for (int q = threadIdx.x; q < k; q += blockDim.x) delta[q] = 0;
+    __syncthreads();
+}
+__device__ __forceinline__ void rb_delta_end(int64_t* delta, int32_t k, int64_t nmoves, int64_t* __restrict__ pw,
+                                             int64_t* __restrict__ moves) {
+    for (int o = 16; o > 0; o >>= 1) nmoves += __shfl_xor_sync(0xffffffffu, nmoves, o);
+    if ((threadIdx.x & 31) == 0 && nmoves) atomicAdd((unsigned long long*)moves, (unsigned long long)nmoves);
+    __syncthreads();
+    for (int q = threadIdx.x; q < k; q += blockDim.x)
+        if (delta[q]) atomicAdd((unsigned long long*)&pw[q], (unsigned long long)delta[q]);
+}
+
 // weak: keep moves whose destination prefix fits the capacity; apply
-__global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, const int32_t* __restrict__ vals,
-                                const int64_t* __restrict__ pre, const int32_t* __restrict__ vw,
-                                const int64_t* __restrict__ pw_snap, int64_t Lmax, int32_t* __restrict__ part,
-                                void* pc, int pcb, uint8_t* __restrict__ lock, int64_t* __restrict__ pw,
-                                int64_t* __restrict__ moves) {
+__global__ void k_rb_weak_apply(int64_t cnt, const uint64_t* __restrict__ keys, const int64_t* __restrict__ segf,
+                                const int32_t* __restrict__ vals, const int64_t* __restrict__ pre,
+                                const int32_t* __restrict__ vw, const int64_t* __restrict__ pw_snap, int64_t Lmax,
+                                int32_t k, int32_t* __restrict__ part, void* pc, int pcb, uint8_t* __restrict__ lock,
+                                int64_t* __restrict__ pw, int64_t* __restrict__ moves) {
+    extern __shared__ int64_t rb_delta[];
+    rb_delta_begin(rb_delta, k);
+    int64_t nm = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t d = keys[i] >> RB_SHIFT;
-        const int64_t s = seg_start(keys, i, d);
+        const int64_t s = segf[d];
         const int32_t v = vals[i];
         const int64_t wv = vw ? vw[v] : 1;
         if ((pre[i] - pre[s]) + wv <= Lmax - pw_snap[d]) {
             const int32_t p = part[v];
             part[v] = (int32_t)d; lock[v] = 1;
             store_pc(pc, pcb, v, (int32_t)d);
-            atomicAdd((unsigned long long*)&pw[d], (unsigned long long)wv);
-            atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
-            atomicAdd((unsigned long long*)moves, 1ull);
+            if (GP_IN(d, k) && GP_IN(p, k)) {
+                atomicAdd((unsigned long long*)&rb_delta[d], (unsigned long long)wv);
+                atomicAdd((unsigned long long*)&rb_delta[p], (unsigned long long)(-wv));
+            }
+            ++nm;
         }
     }
+    rb_delta_end(rb_delta, k, nm, pw, moves);
 }
 
 // strong: cumulative free capacity of non-overweight parts
@@ -859,6 +888,9 @@ __global__ void k_rb_strong_apply(int64_t cnt, const int32_t* __restrict__ vals,
                                   const int64_t* __restrict__ cum, int32_t k, int32_t* __restrict__ part,
                                   void* pc, int pcb, uint8_t* __restrict__ lock, int64_t* __restrict__ pw,
                                   int64_t* __restrict__ moves) {
+    extern __shared__ int64_t rb_delta[];
+    rb_delta_begin(rb_delta, k);
+    int64_t nm = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
         const int64_t pre = P[i];
@@ -876,11 +908,14 @@ __global__ void k_rb_strong_apply(int64_t cnt, const int32_t* __restrict__ vals,
             const int32_t p = part[v];
             part[v] = q; lock[v] = 1;
             store_pc(pc, pcb, v, q);
-            atomicAdd((unsigned long long*)&pw[q], (unsigned long long)wv);
-            atomicAdd((unsigned long long*)&pw[p], (unsigned long long)(-wv));
-            atomicAdd((unsigned long long*)moves, 1ull);
+            if (GP_IN(p, k)) {
+                atomicAdd((unsigned long long*)&rb_delta[q], (unsigned long long)wv);
+                atomicAdd((unsigned long long*)&rb_delta[p], (unsigned long long)(-wv));
+            }
+            ++nm;
         }
     }
+    rb_delta_end(rb_delta, k, nm, pw, moves);
 }
 
 // ------------------------------------------------------------------ projection, weights, cut
@@ -1847,7 +1882,10 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                 k_gather_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, g.vw, wv);
                 GP_LAUNCHED(c);
                 scan_excl_i32_to_i64(c, wv, pre, ncand, nullptr);
-                k_rb_source<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, pre, B.pw, Lmax, acc);
+                int64_t* segf = c.tmp_alloc<int64_t>(k + 1);
+                k_seg_first<<<grid_for(k + 1, 256), 256, 0, c.s>>>(ncand, B.ckeys, k, segf);
+                GP_LAUNCHED(c);
+                k_rb_source<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.ckeys, segf, pre, B.pw, Lmax, acc);
                 GP_LAUNCHED(c);
                 if (mode == 1) {
                     int64_t* apos = c.tmp_alloc<int64_t>(ncand + 1);
@@ -1861,9 +1899,11 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                         k_gather_vw<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.cvals2, g.vw, wv);
                         GP_LAUNCHED(c);
                         scan_excl_i32_to_i64(c, wv, pre, n2, nullptr);
-                        k_rb_weak_apply<<<grid_for(n2, 256), 256, 0, c.s>>>(n2, B.ckeys2, B.cvals2, pre, g.vw, pw_snap,
-                                                                           Lmax, B.part, B.pc, B.pcb, B.lock, B.pw,
-                                                                           moves_d);
+                        k_seg_first<<<grid_for(k + 1, 256), 256, 0, c.s>>>(n2, B.ckeys2, k, segf);
+                        GP_LAUNCHED(c);
+                        k_rb_weak_apply<<<grid_for(n2, 256), 256, sizeof(int64_t) * k, c.s>>>(
+                            n2, B.ckeys2, segf, B.cvals2, pre, g.vw, pw_snap, Lmax, k, B.part, B.pc, B.pcb, B.lock, B.pw,
+                            moves_d);
                         GP_LAUNCHED(c);
                     }
                 } else {
@@ -1874,9 +1914,8 @@ int refine_level(Ctx& c, const Level& L, const Params& P, RefineBufs& B, int lev
                     k_mask_vw<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, acc, wv, wm);
                     GP_LAUNCHED(c);
                     scan_excl_i32_to_i64(c, wm, pre, ncand, nullptr);
-                    k_rb_strong_apply<<<grid_for(ncand, 256), 256, 0, c.s>>>(ncand, B.cvals, acc, pre, g.vw, cum, k,
-                                                                           B.part, B.pc, B.pcb, B.lock, B.pw,
-                                                                           moves_d);
+                    k_rb_strong_apply<<<grid_for(ncand, 256), 256, sizeof(int64_t) * k, c.s>>>(
+                        ncand, B.cvals, acc, pre, g.vw, cum, k, B.part, B.pc, B.pcb, B.lock, B.pw, moves_d);
                     GP_LAUNCHED(c);
                 }
                 c.bytes += 80 * ncand;
