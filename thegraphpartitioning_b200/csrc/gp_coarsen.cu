@@ -205,6 +205,8 @@ struct MatchArgs {
     int2* cand;               // MODE 0, rows of 33+ entries (one piece): the two best eligible
     uint8_t* cmore;           // neighbours of the row's last scan and whether it had more
                               // (nullptr: no cache)
+    int32_t* anchor0;         // the same rows' best neighbour in round 0; with no weight check
+                              // that is the two-hop anchor (MODE 1 reads it instead of scanning)
     const uint8_t* hdead;     // MODE 0: heavy rows left without an eligible neighbour (nullptr: none)
     int any_matched;          // MODE 0: 0 in the first round (no neighbour to look up in match[])
     int check_vw;             // MODE 0: 0 when no two vertices of the level can exceed maxvw
@@ -281,6 +283,10 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
         const int64_t v = A.heavy[h];
         if (A.match[v] != -1 || (A.hdead && A.hdead[h])) { if (MODE == 0 && threadIdx.x == 0) A.out[v] = -1; return; }
         const int nit = A.row_items[h];
+        if (MODE == 1 && A.anchor0 && nit == 1) {
+            if (threadIdx.x < 32) match_emit<MODE>(A, threadIdx.x == 0, v, A.anchor0[v]);
+            return;
+        }
         // a row in one piece keeps its two best eligible neighbours (as the warp rows do)
         const bool cached = MODE == 0 && A.cand && nit == 1;
         if (cached && A.any_matched) {
@@ -327,6 +333,7 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
             if (threadIdx.x == 0) {
                 A.cand[v] = make_int2(s_best, ks ? is : -1);
                 A.cmore[v] = s_cnt > 2 ? 1 : 0;
+                if (!A.any_matched && A.anchor0) A.anchor0[v] = s_best;
                 A.out[v] = s_best;
             }
             return;
@@ -368,6 +375,7 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
             const bool valid = A.match[v] == -1;
             uint64_t bk = 0; int32_t bid = -1;
             bool scan = valid;
+            if (MODE == 1 && valid && A.anchor0) { bid = A.anchor0[v]; scan = false; }
             if (MODE == 0 && valid && A.cand && A.any_matched) {
                 // neighbours only ever become matched, so the best of the row's
                 // last two cached candidates that is still unmatched is its
@@ -423,6 +431,7 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
                     if (lane == 0) {
                         A.cand[v] = make_int2(bid, sk ? si : -1);
                         A.cmore[v] = tot > 2 ? 1 : 0;
+                        if (!A.any_matched && A.anchor0) A.anchor0[v] = bid;
                     }
                 }
             }
@@ -541,6 +550,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     // rows of 33+ entries keep their two best eligible neighbours between rounds (written by round 0)
     A.cand = c.tmp_alloc<int2>(g.n);
     A.cmore = c.tmp_alloc<uint8_t>(g.n);
+    A.anchor0 = c.tmp_alloc<int32_t>(g.n);
     // weight cap: skip the per-neighbour weight check when the two heaviest
     // vertices of the level together stay within maxvw
     A.check_vw = 0;
@@ -559,6 +569,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
     for (int b = 0; b < 3; ++b) { A.list[b] = L.bucket[b]; A.nlist[b] = L.nbucket[b]; }
     int64_t pairs = 0, heavy_live = L.nheavy;
     int rounds = 0;
+    bool anchors_ready = false;   // round 0 ran and wrote anchor0
     for (int r = 0; r < P.o.match_rounds; ++r) {
         const int64_t units = (A.nlist[0] + 3) / 4 + A.nlist[1] + A.nlist[2];
         // nobody left who can propose: this round would add no pair
@@ -568,6 +579,7 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         memset_async(c, d_cnt, 0, 5 * sizeof(int64_t));
         k_match_scan<0><<<grid, 256, 0, c.s>>>(A);
         GP_LAUNCHED(c);
+        if (r == 0) anchors_ready = true;
         int32_t** nxt = wl[r & 1];
         const int64_t tot = A.nlist[0] + A.nlist[1] + A.nlist[2] + L.nheavy;
         k_handshake<<<grid_for(tot, 256), 256, 0, c.s>>>(g.rp, g.n, L.heavy_deg, A.list[0], A.list[1], A.list[2], A.nlist[0], A.nlist[1],
@@ -595,6 +607,8 @@ int64_t match_level(Ctx& c, const Level& L, int level, const Params& P, int32_t*
         MatchArgs B2 = A;
         B2.hdead = nullptr;   // anchors: the top neighbour over all neighbours
         B2.cand = nullptr; B2.cmore = nullptr;
+        // round 0 saw every neighbour but v itself when no pair can exceed the weight cap
+        if (A.check_vw || !anchors_ready) B2.anchor0 = nullptr;
         B2.any_matched = 1;
         for (int b = 0; b < 3; ++b) { B2.list[b] = L.bucket[b]; B2.nlist[b] = L.nbucket[b]; }
         B2.out = nullptr; B2.keys = keys; B2.nkeys = d_cnt + 1; B2.nbits = nb;
