@@ -202,9 +202,9 @@ struct MatchArgs {
     int64_t* nkeys;
     int nbits;
     const int32_t* prio;      // learned priorities per entry (nullptr: edge weights)
-    int2* cand;               // MODE 0, rows of 33+ entries (one piece): the two best eligible
-    uint8_t* cmore;           // neighbours of the row's last scan and whether it had more
-                              // (nullptr: no cache)
+    int2* cand;               // MODE 0, rows of 33+ entries (one piece): the best eligible
+    uint8_t* cmore;           // neighbours of the row's last scan (warp rows: the best; CTA rows:
+                              // the two best) and whether it had more (nullptr: no cache)
     int32_t* anchor0;         // the same rows' best neighbour in round 0; with no weight check
                               // that is the two-hop anchor (MODE 1 reads it instead of scanning)
     const uint8_t* hdead;     // MODE 0: heavy rows left without an eligible neighbour (nullptr: none)
@@ -377,16 +377,16 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
             bool scan = valid;
             if (MODE == 1 && valid && A.anchor0) { bid = A.anchor0[v]; scan = false; }
             if (MODE == 0 && valid && A.cand && A.any_matched) {
-                // neighbours only ever become matched, so the best of the row's
-                // last two cached candidates that is still unmatched is its
-                // best eligible neighbour; with both matched and no third, none
+                // neighbours only ever become matched, so the row's cached best
+                // eligible neighbour, if still unmatched, is its best eligible
+                // neighbour; with it matched and no other eligible entry, none
                 const int2 cc = A.cand[v];
                 const int32_t m1 = cc.x >= 0 ? A.match[cc.x] : 0, m2 = cc.y >= 0 ? A.match[cc.y] : 0;
                 if (cc.x >= 0 && m1 == -1) { bid = cc.x; scan = false; }
                 else if (cc.y >= 0 && m2 == -1) { bid = cc.y; scan = false; }
                 else if (!A.cmore[v]) { bid = -1; scan = false; }
             }
-            uint64_t k2 = 0; int32_t i2 = -1, cnt = 0;
+            int32_t cnt = 0;   // eligible entries
             if (scan) {
                 const int64_t vwv = A.g.vw ? A.g.vw[v] : 1;
                 const int64_t beg = A.g.rp[v], end = A.g.rp[v + 1];
@@ -415,22 +415,18 @@ __global__ void __launch_bounds__(256, 6) k_match_scan(MatchArgs A) {
                         if (x < 0 || x == (int32_t)v) continue;
                         if (MODE == 0 && (mm[c] != -1 || (A.check_vw && vwv + vv[c] > A.maxvw))) continue;
                         const uint64_t key = edge_key(ww[c], edge_hash(A.salt, (int32_t)v, x));
-                        if (MODE == 0 && A.cand) { top2_insert(bk, bid, k2, i2, key, x); ++cnt; }
-                        else argmax_merge(bk, bid, key, x);
+                        argmax_merge(bk, bid, key, x);
+                        if (MODE == 0 && A.cand) ++cnt;
                     }
                 }
-                const uint64_t k1 = bk;
-                const int32_t i1 = bid;
                 warp_argmax(bk, bid);
                 if (MODE == 0 && A.cand) {
-                    // second: each lane offers its best neighbour other than the row's best
-                    uint64_t sk = i1 == bid ? k2 : k1;
-                    int32_t si = i1 == bid ? i2 : i1;
-                    warp_argmax(sk, si);
+                    // warp rows keep the best only (a second candidate costs more in
+                    // round 0 than the rescans it saves)
                     const int32_t tot = (int32_t)__reduce_add_sync(0xffffffffu, (uint32_t)cnt);
                     if (lane == 0) {
-                        A.cand[v] = make_int2(bid, sk ? si : -1);
-                        A.cmore[v] = tot > 2 ? 1 : 0;
+                        A.cand[v] = make_int2(bid, -1);
+                        A.cmore[v] = tot > 1 ? 1 : 0;
                         if (!A.any_matched && A.anchor0) A.anchor0[v] = bid;
                     }
                 }
