@@ -299,8 +299,8 @@ int gp_gnn_move_train_step_device(gp_gnn* model, int64_t ns, const float* d_feat
  * that loads the library until the process exits), so k must not exceed
  * GP_NOALLOC_MAX_K (GP_EINVAL otherwise).  All calls on a device share that
  * array: calls that overlap on the GPU race and must be serialized by the
- * caller.  The first call on each device looks up the array's address; make
- * it before any stream capture.  Synchronizes `stream`. */
+ * caller.  Every call looks up the array's address in the current context.
+ * Synchronizes `stream`. */
 int gp_edge_cut_device_noalloc(int64_t n, const int64_t* d_rowptr, const int32_t* d_colidx,
                                const int32_t* d_ewgt, const int32_t* d_vwgt,
                                const int32_t* d_part, int32_t k, void* stream,

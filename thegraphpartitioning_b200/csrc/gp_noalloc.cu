@@ -16,14 +16,14 @@
 // * every call on a device shares that one array; calls whose work overlaps
 //   on the GPU (different streams, or several host threads) race and give
 //   wrong results -- serialize them;
-// * the first call on each device looks up the array's device address
-//   (cudaGetSymbolAddress); make that first call before any stream capture;
+// * every call looks up the array's device address (cudaGetSymbolAddress:
+//   no allocation, no stream work), so a device reset or another context
+//   never leaves a stale address behind;
 // * no cudaMalloc, cudaFree, cudaMallocHost or other allocating routine is
 //   called; results are copied into the caller's host memory.
 #define GP_TU_ID 6   // site ids of the bounds-checked build
 #include "gp_internal.cuh"
 
-#include <mutex>
 
 namespace gp {
 
@@ -67,20 +67,14 @@ __global__ void __launch_bounds__(256) k_na_cut(int64_t n, const int64_t* __rest
         if (s_pw[q]) atomicAdd(&acc[1 + q], s_pw[q]);
 }
 
-// device address of the scratch array, looked up once per device
-static unsigned long long* noalloc_scratch(int dev) {
-    static std::mutex mu;
-    static unsigned long long* ptr[64] = {};
-    if (dev < 0 || dev >= 64) throw GpError(GP_EINVAL, "device index out of range");
-    std::lock_guard<std::mutex> lk(mu);
-    if (!ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            throw GpError(GP_ECUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(e));
-        ptr[dev] = (unsigned long long*)p;
-    }
-    return ptr[dev];
+// device address of the scratch array in the current context (looked up on
+// every call: the module may have been reloaded at another address)
+static unsigned long long* noalloc_scratch() {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        throw GpError(GP_ECUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(e));
+    return (unsigned long long*)p;
 }
 
 }  // namespace gp
@@ -105,7 +99,7 @@ extern "C" int gp_edge_cut_device_noalloc(int64_t n, const int64_t* d_rowptr, co
         if (!d_rowptr || !d_colidx || !d_part) throw GpError(GP_EINVAL, "null array");
         int dev = 0;
         GP_CUDA(cudaGetDevice(&dev));
-        unsigned long long* scratch = noalloc_scratch(dev);
+        unsigned long long* scratch = noalloc_scratch();
         unsigned long long* err = scratch + 1 + GP_NOALLOC_MAX_K;
         cudaStream_t s = (cudaStream_t)stream;
         int sms = 148;
