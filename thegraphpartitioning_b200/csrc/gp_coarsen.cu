@@ -1012,6 +1012,28 @@ __global__ void __launch_bounds__(T) k_dedup_cta_smem(DGraph g, const int32_t* _
     }
 }
 
+// rows of a one-CTA-per-row tier, longest walk first: the block scheduler
+// starts CTAs in list order, so the long rows no longer trail the launch
+__global__ void k_len_keys(const int32_t* __restrict__ list, int64_t nlist, const int64_t* __restrict__ cdeg,
+                           int64_t maxrow, uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nlist; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = list[i];
+        const int64_t d = cdeg[c];
+        keys[i] = (uint64_t)(d < maxrow ? maxrow - d : 0);
+        vals[i] = c;
+    }
+}
+static int32_t* longest_first(Ctx& c, const int32_t* list, int64_t nlist, const int64_t* cdeg, int64_t maxrow) {
+    uint64_t* keys = c.tmp_alloc<uint64_t>(nlist);
+    uint64_t* keys2 = c.tmp_alloc<uint64_t>(nlist);
+    int32_t* vals = c.tmp_alloc<int32_t>(nlist);
+    int32_t* vals2 = c.tmp_alloc<int32_t>(nlist);
+    k_len_keys<<<grid_for(nlist, 256), 256, 0, c.s>>>(list, nlist, cdeg, maxrow, keys, vals);
+    GP_LAUNCHED(c);
+    radix_sort_pairs(c, keys, vals, keys2, vals2, nlist, bits_for(maxrow + 1));
+    return vals;
+}
+
 // tier C3: one 1024-thread CTA per row of TC2_ROW < d <= TC3_ROW walk entries.
 // Pass 0 gathers the walk through cmap once and leaves the mapped ids and
 // weights in the row's range of the scratch arrays (key_at, w_at); passes
@@ -1425,6 +1447,8 @@ void contract_level(Ctx& c, Level& fine, Level& coarse, const int32_t* match) {
                                                           err);
         GP_LAUNCHED(c);
     }
+    if (nC2 > c.sm_count) listC2 = longest_first(c, listC2, nC2, cdeg, TC2_ROW);
+    if (nC3 > c.sm_count) listC3 = longest_first(c, listC3, nC3, cdeg, TC3_ROW);
     if (nC2 > 0) {
         k_dedup_cta_smem<TC2_T, TC2_SLOTS, TC2_ROW>
             <<<(unsigned)std::min<int64_t>(nC2, (int64_t)c.sm_count * c.ctas_per_sm), TC2_T,
