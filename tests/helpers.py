@@ -42,6 +42,38 @@ def star_plus_grid(leaves=3000, side=24):
     return rp2, ci2
 
 
+def multi_star_grid(hub_leaves=(700, 3000, 9000, 30000, 90000), side=32, shared=0.2, seed=0):
+    """Hubs of the given leaf counts on a grid, so that the first coarse level
+    has rows in every contraction tier (walks of about 700, 3,000, 9,000,
+    30,000 and 90,000 entries); each hub also links to a `shared` fraction of
+    the previous hub's leaves, so that coarse walks hold repeated neighbours."""
+    rng = np.random.default_rng(seed)
+    rp, ci = graphs.grid2d(side, side)
+    g = side * side
+    src = [np.repeat(np.arange(g), np.diff(rp.numpy()))]
+    dst = [ci.numpy().astype(np.int64)]
+    nxt = g
+    prev = None
+    for i, nl in enumerate(hub_leaves):
+        hub = nxt
+        leaf = np.arange(hub + 1, hub + 1 + nl)
+        nxt = hub + 1 + nl
+        att = np.array([i % g])
+        src += [np.full(nl, hub), leaf, np.array([hub]), att]
+        dst += [leaf, np.full(nl, hub), att, np.array([hub])]
+        src += [leaf[:-1:5], leaf[1::5]]          # chains among the leaves
+        dst += [leaf[1::5], leaf[:-1:5]]
+        if prev is not None:
+            extra = rng.choice(prev, size=int(shared * len(prev)), replace=False)
+            src += [np.full(len(extra), hub), extra]
+            dst += [extra, np.full(len(extra), hub)]
+        prev = leaf
+    s = torch.from_numpy(np.concatenate(src).astype(np.int64))
+    d = torch.from_numpy(np.concatenate(dst).astype(np.int64))
+    rp2, ci2, _ = graphs.csr_from_edges(s, d, nxt)
+    return rp2, ci2
+
+
 def weighted(rp, ci, seed=0, wmax=9):
     """Symmetric random integer edge weights in [1, wmax] and vertex weights in [1, 4]."""
     rp = np.asarray(rp); ci = np.asarray(ci)

@@ -11,7 +11,7 @@ import pytest
 import torch
 
 from thegraphpartitioning_b200 import graphs
-from helpers import compare_traces, star_plus_grid, to_np, weighted
+from helpers import compare_traces, multi_star_grid, star_plus_grid, to_np, weighted
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +29,9 @@ def _cases():
     yield "megahub_w_k3", star_plus_grid(leaves=36000, side=40), 3, 0.05, "w", {"coarsen_to": 300}
     # a 150000-leaf hub: its coarse row is contracted by several CTAs sharing one table
     yield "gigahub_k4", star_plus_grid(leaves=150000, side=32), 4, 0.03, None, {}
+    # hubs of 700 to 90,000 leaves: coarse rows in every contraction tier (C1, C, C2, C3, D)
+    yield "multistar_k8", multi_star_grid(), 8, 0.03, None, {}
+    yield "multistar_w_k5", multi_star_grid(seed=1), 5, 0.05, "w", {}
     yield "rmat11_k64_tight", graphs.rmat(11, seed=3)[:2], 64, 0.0, None, {}
     yield "er_k3_nohop", graphs.erdos_renyi(3000, 3.0, seed=5), 3, 0.02, None, {"two_hop": -1}
     yield "rgg_k2", graphs.random_geometric(4000, 8.0, seed=6), 2, 0.03, None, {"init_trials": 8}
