@@ -23,7 +23,7 @@ sys.path.insert(0, ROOT); sys.path.insert(0, ROOT + "/tests")
 import oracle
 import thegraphpartitioning_b200 as gp
 from thegraphpartitioning_b200 import graphs
-from helpers import star_plus_grid, to_np, weighted
+from helpers import multi_star_grid, star_plus_grid, to_np, weighted
 assert gp.CHECKED and gp.LIB_PATH.endswith("libgp_b200_checked.so")
 assert "bounds-checked" in gp.version()
 dev = torch.device("cuda:0")
@@ -33,6 +33,7 @@ cases = [
     (to_np(*graphs.chung_lu(30000, 100000, seed=2)), 8, {}),
     (to_np(*star_plus_grid(leaves=40000, side=64)), 4, {}),
     (to_np(*star_plus_grid(leaves=150000, side=32)), 3, {}),
+    (to_np(*multi_star_grid()), 8, {}),
     (to_np(*graphs.grid3d(20, 20, 20)), 32, {"small_level_n": 16384}),
     (to_np(*graphs.random_geometric(50000, 8.0, seed=9)), 2, {}),
     (to_np(*graphs.rmat(12, seed=3)[:2]), 16, {"heavy_deg": 64, "item_len": 96}),
