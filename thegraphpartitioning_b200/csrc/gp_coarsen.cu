@@ -683,7 +683,7 @@ __global__ void k_cmap(DGraph g, const int32_t* __restrict__ match, const int64_
 //   C3 d <= 65536      one 1024-thread CTA, the C2 table in P = 2..8 passes: pass p
 //                      dedups the keys whose pass hash is p, first positions are
 //                      marked in a shared-memory bitmap of the whole walk
-//   D  longer          pieces of 64K entries, one CTA each, table in global memory
+//   D  longer          pieces of 16K entries, one CTA each, table in global memory
 // A and B insert 32 entries at a time in walk order (match_any leaders), so
 // new neighbours get consecutive ranks; C and D rank first positions with one
 // block scan over per-thread contiguous segments.  The on-chip tables are
@@ -1178,7 +1178,7 @@ __global__ void __launch_bounds__(TC2_T) k_dedup_multipass(DGraph g, const int32
 // popcounts ranks the words of every row, D3 writes the first occurrences at
 // their ranks.  Same output as one CTA per row: unique neighbours in order of
 // first occurrence with summed weights.
-constexpr int64_t TD_PIECE = 65536;   // multiple of 32
+constexpr int64_t TD_PIECE = 16384;   // multiple of 32
 struct TierD {
     const int32_t* rc;      // coarse row of each tier-D row
     const int32_t* rlg;     // log2 of its table size
