@@ -526,7 +526,7 @@ void refine_level(const Graph& g, std::vector<int32_t>& part, const Params& P, i
                 }
             }
             if (mode == 1) {
-                std::vector<Cand> bd = acc;
+                std::vector<Cand>& bd = acc;   // accepted moves, re-sorted by destination (acc is not used again)
                 std::sort(bd.begin(), bd.end(), [](const Cand& a, const Cand& b) {
                     if (a.d != b.d) return a.d < b.d;
                     if (a.bucket != b.bucket) return a.bucket < b.bucket;
